@@ -1,0 +1,235 @@
+// image.cu -- exact uv-gridding of the integrated cube and a batched
+// shared-memory 2-D FFT.
+//
+// mixer_grid replaces k_grid_cube (reference src/rx_host_corr.cu:79-85): the
+// reference scatters every ordered pair (a, b) of the FP32 cube with float
+// atomicAdd, so its sum depends on the order of the atomics.  Here each CTA
+// owns one (channel, lower-triangle tile), accumulates int64 sums in a small
+// shared-memory window of the baseline offsets that tile can reach, and adds
+// window cell S(d) to grid cell d and conj(S(d)) to cell -d with int64
+// atomics: the pair (b, a) carries conj(V[a][b]), so this equals the
+// full-square sum exactly, in any order.
+//
+// mixer_image_fft replaces cufftPlanMany/cufftExecC2C (src/rx_host_corr.cu:
+// 205-206,222) plus the host fftshift / real part / min-max loop (:230-235):
+// one CTA per channel loads the int64 grid as complex FP32 in bit-reversed
+// order, runs radix-2 butterflies along rows then columns in shared memory
+// with twiddles generated in FP64, and writes Re(F) shifted by G/2 in both
+// axes together with the channel's max and min.
+#include "common.cuh"
+
+namespace mixer {
+namespace {
+
+__device__ __forceinline__ void decode_tile_g(int t, int& i, int& j) {
+    int ii = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
+    while ((ii + 1) * (ii + 2) / 2 <= t) ++ii;
+    while (ii * (ii + 1) / 2 > t) --ii;
+    i = ii;
+    j = t - ii * (ii + 1) / 2;
+}
+
+__host__ __device__ inline int floordiv(int a, int b) { return a / b; }   // a >= 0
+
+__host__ __device__ inline void tile_window(int i, int j, int nant, int sx, int& dylo, int& ny) {
+    const int a0 = 128 * i, a1 = min(128 * i + 128, nant) - 1;
+    const int b0 = 128 * j, b1 = min(128 * j + 128, nant) - 1;
+    dylo = floordiv(a0, sx) - floordiv(b1, sx);
+    const int dyhi = floordiv(a1, sx) - floordiv(b0, sx);
+    ny = dyhi - dylo + 1;
+}
+
+__device__ __forceinline__ int pmod(int v, int g) {
+    const int r = v % g;
+    return r < 0 ? r + g : r;
+}
+
+// grid: x = tile, y = channel.  smem: window [ny][2 sx - 1][2] int64.
+__global__ void __launch_bounds__(256)
+    k_grid_tiles(const long long* __restrict__ vis, int nant, int ntiles, int sx, int G,
+                 unsigned long long* __restrict__ grid) {
+    extern __shared__ unsigned long long win[];
+    __shared__ unsigned long long diag[2];
+    const int t = blockIdx.x, c = blockIdx.y;
+    int i, j;
+    decode_tile_g(t, i, j);
+    int dylo, ny;
+    tile_window(i, j, nant, sx, dylo, ny);
+    const int nx = 2 * sx - 1;
+    const int ncell = ny * nx;
+    for (int q = threadIdx.x; q < 2 * ncell; q += blockDim.x) win[q] = 0ull;
+    if (threadIdx.x < 2) diag[threadIdx.x] = 0ull;
+    __syncthreads();
+
+    const long long* re = vis + (((size_t)c * ntiles + t) * 2) * 16384;
+    const long long* im = re + 16384;
+    for (int e = threadIdx.x; e < 16384; e += blockDim.x) {
+        const int n = e >> 7, m = e & 127;
+        const int a = 128 * i + m, b = 128 * j + n;
+        if (a >= nant || b >= nant) continue;
+        if (i == j && m < n) continue;           // upper half of a diagonal tile
+        const long long vr = re[e], vi = im[e];
+        if (a == b) {
+            atomicAdd(&diag[0], (unsigned long long)vr);
+            atomicAdd(&diag[1], (unsigned long long)vi);
+            continue;
+        }
+        const int dy = a / sx - b / sx, dx = a % sx - b % sx;
+        const int cell = (dy - dylo) * nx + (dx + sx - 1);
+        atomicAdd(&win[2 * cell + 0], (unsigned long long)vr);
+        atomicAdd(&win[2 * cell + 1], (unsigned long long)vi);
+    }
+    __syncthreads();
+    unsigned long long* gc = grid + (size_t)c * G * G * 2;
+    for (int q = threadIdx.x; q < ncell; q += blockDim.x) {
+        const unsigned long long sr = win[2 * q], si = win[2 * q + 1];
+        if (sr == 0ull && si == 0ull) continue;
+        const int dy = q / nx + dylo, dx = q % nx - (sx - 1);
+        const int f = pmod(dy, G) * G + pmod(dx, G);
+        const int r = pmod(-dy, G) * G + pmod(-dx, G);
+        atomicAdd(&gc[2 * f + 0], sr);
+        atomicAdd(&gc[2 * f + 1], si);
+        atomicAdd(&gc[2 * r + 0], sr);
+        atomicAdd(&gc[2 * r + 1], (unsigned long long)(-(long long)si));
+    }
+    if (threadIdx.x == 0 && (diag[0] | diag[1])) {
+        atomicAdd(&gc[0], diag[0]);
+        atomicAdd(&gc[1], diag[1]);
+    }
+}
+
+// grid = grid - prev, prev = old grid (delta imaging), n int64 values.
+__global__ void k_grid_delta(long long* __restrict__ grid, long long* __restrict__ prev, int64_t n) {
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        const long long g = grid[q];
+        grid[q] = g - prev[q];
+        prev[q] = g;
+    }
+}
+
+__global__ void __launch_bounds__(512)
+    k_image_fft(const long long* __restrict__ grid, int G, int logG, float* __restrict__ img,
+                float* __restrict__ vmax, float* __restrict__ vmin) {
+    extern __shared__ float2 S[];               // [G][G] then twiddles [G/2]
+    float2* tw = S + G * G;
+    __shared__ float red_max[16], red_min[16];
+    const int c = blockIdx.x;
+    const int GG = G * G, H = G / 2;
+    // twiddles W_G^k = exp(-2 pi i k / G), generated in FP64
+    for (int k = threadIdx.x; k < H; k += blockDim.x) {
+        double sn, cs;
+        sincospi(2.0 * (double)k / (double)G, &sn, &cs);
+        tw[k] = make_float2((float)cs, (float)(-sn));
+    }
+    const long long* g = grid + (size_t)c * GG * 2;
+    const int sh = 32 - logG;
+    for (int q = threadIdx.x; q < GG; q += blockDim.x) {
+        const int y = q / G, x = q - y * G;
+        const int yb = (int)(__brev((unsigned)y) >> sh), xb = (int)(__brev((unsigned)x) >> sh);
+        S[yb * G + xb] = make_float2(__ll2float_rn(g[2 * q]), __ll2float_rn(g[2 * q + 1]));
+    }
+    __syncthreads();
+    // pass 0: along x (within rows); pass 1: along y (within columns)
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int s = 0; s < logG; ++s) {
+            const int h = 1 << s;
+            const int tstride = H >> s;          // twiddle index step
+            for (int bf = threadIdx.x; bf < G * H; bf += blockDim.x) {
+                const int line = bf / H, r = bf - line * H;
+                const int jj = r & (h - 1), blk = r >> s;
+                const int i0 = blk * 2 * h + jj, i1 = i0 + h;
+                const int a0 = pass == 0 ? line * G + i0 : i0 * G + line;
+                const int a1 = pass == 0 ? line * G + i1 : i1 * G + line;
+                const float2 w = tw[jj * tstride];
+                const float2 u = S[a0], v = S[a1];
+                const float2 vw = make_float2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x);
+                S[a0] = make_float2(u.x + vw.x, u.y + vw.y);
+                S[a1] = make_float2(u.x - vw.x, u.y - vw.y);
+            }
+            __syncthreads();
+        }
+    }
+    float mx = -3.4e38f, mn = 3.4e38f;
+    float* out = img + (size_t)c * GG;
+    for (int q = threadIdx.x; q < GG; q += blockDim.x) {
+        const int y = q / G, x = q - y * G;
+        const float v = S[((y + H) & (G - 1)) * G + ((x + H) & (G - 1))].x;
+        out[q] = v;
+        mx = fmaxf(mx, v);
+        mn = fminf(mn, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red_max[threadIdx.x >> 5] = mx;
+        red_min[threadIdx.x >> 5] = mn;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            mx = fmaxf(mx, red_max[w]);
+            mn = fminf(mn, red_min[w]);
+        }
+        if (vmax) vmax[c] = mx;
+        if (vmin) vmin[c] = mn;
+    }
+}
+
+}  // namespace
+}  // namespace mixer
+
+extern "C" int mixer_grid(const int64_t* vis64, int32_t nant, int32_t nch, int32_t side_x,
+                          int32_t G, int64_t* grid, int64_t* prev, void* stream) {
+    if (!vis64 || !grid || nant <= 0 || nch <= 0 || side_x <= 0 || G <= 0) return MIXER_EINVAL;
+    if (nch > 65535 || G > 4096) return MIXER_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nt = mixer_vis_tiles(nant);
+    int maxcells = 0;
+    for (int t = 0, i = 0; i * 128 < nant; ++i)
+        for (int j = 0; j <= i; ++j, ++t) {
+            int dylo, ny;
+            mixer::tile_window(i, j, nant, side_x, dylo, ny);
+            const int cells = ny * (2 * side_x - 1);
+            if (cells > maxcells) maxcells = cells;
+        }
+    const size_t smem = (size_t)maxcells * 16;
+    if (smem > 200 * 1024) return MIXER_EINVAL;
+    if (smem > 48 * 1024)
+        MIXER_CK(cudaFuncSetAttribute(mixer::k_grid_tiles,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t gbytes = (size_t)nch * G * G * 2 * sizeof(int64_t);
+    MIXER_CK(cudaMemsetAsync(grid, 0, gbytes, st));
+    dim3 g((unsigned)nt, (unsigned)nch);
+    mixer::k_grid_tiles<<<g, 256, smem, st>>>(reinterpret_cast<const long long*>(vis64), nant, nt,
+                                              side_x, G,
+                                              reinterpret_cast<unsigned long long*>(grid));
+    MIXER_CK(cudaGetLastError());
+    if (prev) {
+        const int64_t n = (int64_t)nch * G * G * 2;
+        int64_t blocks = (n + 255) / 256;
+        if (blocks > 4096) blocks = 4096;
+        mixer::k_grid_delta<<<(unsigned)blocks, 256, 0, st>>>(reinterpret_cast<long long*>(grid),
+                                                              reinterpret_cast<long long*>(prev), n);
+        MIXER_CK(cudaGetLastError());
+    }
+    return MIXER_OK;
+}
+
+extern "C" int mixer_image_fft(const int64_t* grid, int32_t nch, int32_t G, float* img, float* vmax,
+                               float* vmin, void* stream) {
+    if (!grid || !img || nch <= 0) return MIXER_EINVAL;
+    int logG = 0;
+    while ((1 << logG) < G) ++logG;
+    if ((1 << logG) != G || G < 4 || G > 128) return MIXER_EINVAL;
+    const size_t smem = (size_t)G * G * sizeof(float2) + (size_t)(G / 2) * sizeof(float2);
+    if (smem > 48 * 1024)
+        MIXER_CK(cudaFuncSetAttribute(mixer::k_image_fft,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    mixer::k_image_fft<<<(unsigned)nch, 512, smem, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const long long*>(grid), G, logG, img, vmax, vmin);
+    MIXER_CK(cudaGetLastError());
+    return MIXER_OK;
+}

@@ -1,0 +1,389 @@
+// xcorr.cu -- lower-triangle complex Hermitian GEMM V = X X^H per channel on
+// tcgen05 int8 tensor cores (sm_100a).
+//
+// Replaces cgemm_blk_t<ACC> (reference src/cgemm.cuh:28-69).  The reference
+// issues four wmma 16x16x16 products per tile from global memory, negates the
+// A_im fragment (src/cgemm.cuh:52, wraps for -128) and computes the full
+// square.  Here, per channel c and 128 x 128 tile (i, j) with j <= i:
+//
+//   acc_re += Xr_i Xr_j^T + Xi_i Xi_j^T          (TMEM columns   0..127)
+//   acc_p1 += Xi_i Xr_j^T                        (TMEM columns 128..255)
+//   acc_p2 += Xr_i Xi_j^T                        (TMEM columns 256..383)
+//   Re V = acc_re,  Im V = acc_p1 - acc_p2       (epilogue)
+//
+// so no operand is ever negated and every int8 input, -128 included, is exact.
+// Operands come from the corner-turned planes [2][C][N][kt] through 4-D TMA
+// tensor loads (128-byte swizzle, 128 x 128-byte boxes), staged in a 3-deep
+// shared-memory ring.  One elected thread issues all tcgen05.mma; int32
+// accumulators live in TMEM for the whole K range of the launch; four
+// epilogue warps read them back with tcgen05.ld and add them into the
+// tile-packed int32 or int64 cube in HBM.
+//
+// Warp roles (192 threads, one CTA per SM, persistent over work items):
+//   warp 0      TMA producer
+//   warp 1      TMEM allocator + MMA issuer
+//   warps 2..5  epilogue (TMEM lane quadrant = warp % 4)
+#include "common.cuh"
+
+namespace mixer {
+
+namespace {
+
+constexpr int kTile = 128;                       // tile rows = cols
+constexpr int kKc = 128;                         // samples (bytes) per stage
+constexpr int kStages = 3;
+constexpr int kTileBytes = kTile * kKc;          // 16 KiB
+constexpr int kStageBytes = 4 * kTileBytes;      // Ar, Ai, Br, Bi
+constexpr int kBarBytes = 256;
+constexpr int kSmemBytes = kStages * kStageBytes + 1024 + kBarBytes;
+constexpr uint32_t kTmemCols = 512;              // 3 x 128 used
+constexpr uint32_t kIdesc = idesc_i8(128, 128);
+
+struct XcorrArgs {
+    int32_t nant, nch, nblk, ntiles;
+    int32_t kbeg, nkc;   // first sample, number of 128-sample chunks
+    int32_t mode;
+    int32_t pad_;
+    int64_t nwork;       // nch * ntiles
+    void* vis;
+    int32_t* err;
+};
+
+__device__ __forceinline__ void decode_tile(int t, int& i, int& j) {
+    int ii = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
+    while ((ii + 1) * (ii + 2) / 2 <= t) ++ii;
+    while (ii * (ii + 1) / 2 > t) --ii;
+    i = ii;
+    j = t - ii * (ii + 1) / 2;
+}
+
+// Three 32x32b.x16 TMEM loads (re, p1, p2 columns) and the wait, in one asm
+// statement so no use of the results can be scheduled before the wait.
+__device__ __forceinline__ void tmem_ld3_x16(uint32_t a0, uint32_t a1, uint32_t a2,
+                                             uint32_t (&r)[16], uint32_t (&p)[16],
+                                             uint32_t (&q)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%48];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%49];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47}, [%50];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(p[0]), "=r"(p[1]), "=r"(p[2]), "=r"(p[3]), "=r"(p[4]),
+          "=r"(p[5]), "=r"(p[6]), "=r"(p[7]), "=r"(p[8]), "=r"(p[9]), "=r"(p[10]), "=r"(p[11]),
+          "=r"(p[12]), "=r"(p[13]), "=r"(p[14]), "=r"(p[15]), "=r"(q[0]), "=r"(q[1]), "=r"(q[2]),
+          "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7]), "=r"(q[8]), "=r"(q[9]),
+          "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]), "=r"(q[15])
+        : "r"(a0), "r"(a1), "r"(a2)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(192, 1)
+    k_xcorr_tri(const __grid_constant__ CUtensorMap tmap, const XcorrArgs args) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;           // 1 KiB aligned for SW128
+    uint8_t* gbase = smem_raw + (base - raw);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + kStages * kStageBytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 4);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int FULL = 0, EMPTY = kStages, ACCF = 2 * kStages, ACCE = 2 * kStages + 1,
+              DRAIN = 2 * kStages + 2;
+    auto bar = [&](int k) { return smem_u32(&bars[k]); };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(bar(FULL + s), 1);
+            mbar_init(bar(EMPTY + s), 1);
+        }
+        mbar_init(bar(ACCF), 1);
+        mbar_init(bar(ACCE), 128);
+        mbar_init(bar(DRAIN), 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    if (warp == 0 && lane == 0) prefetch_tmap(&tmap);
+    if (warp == 1) {
+        tmem_alloc(smem_u32(tmem_slot), kTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int64_t issued = 0;
+            bool ok = true;
+            for (int64_t w = blockIdx.x; w < args.nwork && ok; w += gridDim.x) {
+                const int c = (int)(w / args.ntiles);
+                const int t = (int)(w - (int64_t)c * args.ntiles);
+                int i, j;
+                decode_tile(t, i, j);
+                const bool diag = (i == j);
+                const uint32_t bytes = diag ? 2 * kTileBytes : 4 * kTileBytes;
+                for (int kc = 0; kc < args.nkc; ++kc) {
+                    if (!mbar_wait(bar(EMPTY + stage), phase ^ 1u, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t sb = base + stage * kStageBytes;
+                    const uint32_t fb = bar(FULL + stage);
+                    mbar_expect_tx(fb, bytes);
+                    const int k = args.kbeg + kc * kKc;
+                    tma_load_4d(sb + 0 * kTileBytes, &tmap, fb, k, i * kTile, c, 0);
+                    tma_load_4d(sb + 1 * kTileBytes, &tmap, fb, k, i * kTile, c, 1);
+                    if (!diag) {
+                        tma_load_4d(sb + 2 * kTileBytes, &tmap, fb, k, j * kTile, c, 0);
+                        tma_load_4d(sb + 3 * kTileBytes, &tmap, fb, k, j * kTile, c, 1);
+                    }
+                    ++issued;
+                    if (++stage == kStages) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+            }
+            if (!ok) {
+                if (args.err) atomicOr(args.err, 1);
+                *abort_flag = 1;
+                // Let the copies already issued land before the CTA exits.
+                for (int64_t q = issued - 1; q >= 0 && q >= issued - kStages; --q)
+                    mbar_wait(bar(FULL + (int)(q % kStages)), (uint32_t)((q / kStages) & 1));
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0, acc_phase = 0;
+            bool ok = true;
+            const uint32_t t_re = tmem, t_p1 = tmem + 128, t_p2 = tmem + 256;
+            for (int64_t w = blockIdx.x; w < args.nwork; w += gridDim.x) {
+                const int c = (int)(w / args.ntiles);
+                const int t = (int)(w - (int64_t)c * args.ntiles);
+                int i, j;
+                decode_tile(t, i, j);
+                const bool diag = (i == j);
+                if (!mbar_wait(bar(ACCE), acc_phase ^ 1u, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                for (int kc = 0; kc < args.nkc; ++kc) {
+                    if (!mbar_wait(bar(FULL + stage), phase, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sb = base + stage * kStageBytes;
+                    const uint64_t ar = sdesc_sw128(sb);
+                    const uint64_t ai = sdesc_sw128(sb + kTileBytes);
+                    const uint64_t br = diag ? ar : sdesc_sw128(sb + 2 * kTileBytes);
+                    const uint64_t bi = diag ? ai : sdesc_sw128(sb + 3 * kTileBytes);
+#pragma unroll
+                    for (int kk = 0; kk < kKc / 32; ++kk) {
+                        const uint64_t o = (uint64_t)((kk * 32) >> 4);   // 32-byte K step
+                        const uint32_t acc = (kc > 0 || kk > 0) ? 1u : 0u;
+                        mma_i8(t_re, ar + o, br + o, kIdesc, acc);
+                        mma_i8(t_re, ai + o, bi + o, kIdesc, 1u);
+                        mma_i8(t_p1, ai + o, br + o, kIdesc, acc);
+                        mma_i8(t_p2, ar + o, bi + o, kIdesc, acc);
+                    }
+                    tc_commit(bar(EMPTY + stage));   // stage free once these MMAs finish
+                    if (++stage == kStages) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                tc_commit(bar(ACCF));                // accumulators complete
+                acc_phase ^= 1u;
+            }
+            if (!ok) {
+                if (args.err) atomicOr(args.err, 2);
+                *abort_flag = 1;
+            }
+            // No MMA may still be writing TMEM when it is released.
+            tc_commit(bar(DRAIN));
+            mbar_wait(bar(DRAIN), 0);
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue
+        const int q = warp & 3;                      // TMEM lanes 32q .. 32q+31
+        const int m = q * 32 + lane;                 // tile row
+        const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
+        uint32_t acc_phase = 0;
+        for (int64_t w = blockIdx.x; w < args.nwork; w += gridDim.x) {
+            const int c = (int)(w / args.ntiles);
+            const int t = (int)(w - (int64_t)c * args.ntiles);
+            if (!mbar_wait(bar(ACCF), acc_phase, abort_flag)) {
+                if (args.err) atomicOr(args.err, 4);
+                *abort_flag = 1;
+                break;
+            }
+            tc_fence_after();
+            const size_t tb = ((size_t)c * args.ntiles + t) * (size_t)(2 * kTile * kTile);
+#pragma unroll 1
+            for (int n0 = 0; n0 < kTile; n0 += 16) {
+                uint32_t re[16], p1[16], p2[16];
+                tmem_ld3_x16(trow + n0, trow + 128 + n0, trow + 256 + n0, re, p1, p2);
+                if (n0 == kTile - 16) {              // all of this tile's TMEM is read
+                    tc_fence_before();
+                    mbar_arrive(bar(ACCE));
+                }
+                const size_t e0 = tb + (size_t)n0 * kTile + m;
+                if (args.mode == MIXER_VIS_ACC_I64) {
+                    unsigned long long* v = reinterpret_cast<unsigned long long*>(args.vis);
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        const int32_t vr = (int32_t)re[e];
+                        const int32_t vi = (int32_t)(p1[e] - p2[e]);
+                        atomicAdd(v + e0 + (size_t)e * kTile, (unsigned long long)(long long)vr);
+                        atomicAdd(v + e0 + (size_t)e * kTile + kTile * kTile,
+                                  (unsigned long long)(long long)vi);
+                    }
+                } else if (args.mode == MIXER_VIS_ACC_I32) {
+                    int* v = reinterpret_cast<int*>(args.vis);
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        atomicAdd(v + e0 + (size_t)e * kTile, (int)re[e]);
+                        atomicAdd(v + e0 + (size_t)e * kTile + kTile * kTile,
+                                  (int)(p1[e] - p2[e]));
+                    }
+                } else {
+                    int* v = reinterpret_cast<int*>(args.vis);
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        v[e0 + (size_t)e * kTile] = (int)re[e];
+                        v[e0 + (size_t)e * kTile + kTile * kTile] = (int)(p1[e] - p2[e]);
+                    }
+                }
+            }
+            acc_phase ^= 1u;
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        tmem_dealloc(tmem, kTmemCols);
+    }
+}
+
+using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                              const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                              const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeFn get_encode() {
+    static EncodeFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeFn>(p);
+    }
+    return fn;
+}
+
+int sm_count() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 148;
+    return n > 0 ? n : 148;
+}
+
+}  // namespace
+
+// Launch over samples [kbeg, kbeg + klen) with klen <= MIXER_KMAX_I32.
+static int xcorr_launch(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt, int64_t kbeg,
+                        int64_t klen, int32_t mode, void* vis, int32_t* err, cudaStream_t st) {
+    EncodeFn enc = get_encode();
+    if (!enc) return MIXER_ECUDA;
+    CUtensorMap map;
+    // dim 0 ends at kbeg + klen so the last chunk reads zeros past the range.
+    const cuuint64_t dims[4] = {(cuuint64_t)(kbeg + klen), (cuuint64_t)nant, (cuuint64_t)nch, 2};
+    const cuuint64_t strides[3] = {(cuuint64_t)kt, (cuuint64_t)kt * nant,
+                                   (cuuint64_t)kt * nant * nch};
+    const cuuint32_t box[4] = {kKc, kTile, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<int8_t*>(planes), dims,
+                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return MIXER_EINVAL;
+
+    static uint64_t attr_set = 0;   // one bit per device ordinal
+    int dev = 0;
+    MIXER_CK(cudaGetDevice(&dev));
+    if (dev < 64 && !(attr_set & (1ull << dev))) {
+        MIXER_CK(cudaFuncSetAttribute(k_xcorr_tri, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      kSmemBytes));
+        attr_set |= 1ull << dev;
+    }
+    XcorrArgs a;
+    a.nant = nant;
+    a.nch = nch;
+    a.nblk = (nant + kTile - 1) / kTile;
+    a.ntiles = a.nblk * (a.nblk + 1) / 2;
+    a.kbeg = (int32_t)kbeg;
+    a.nkc = (int32_t)((klen + kKc - 1) / kKc);
+    a.mode = mode;
+    a.pad_ = 0;
+    a.nwork = (int64_t)nch * a.ntiles;
+    a.vis = vis;
+    a.err = err;
+    const int64_t grid = a.nwork < sm_count() ? a.nwork : sm_count();
+    k_xcorr_tri<<<(unsigned)grid, 192, kSmemBytes, st>>>(map, a);
+    MIXER_CK(cudaGetLastError());
+    return MIXER_OK;
+}
+
+}  // namespace mixer
+
+extern "C" int32_t mixer_vis_tiles(int32_t nant) {
+    if (nant <= 0) return 0;
+    const int32_t nb = (nant + 127) / 128;
+    return nb * (nb + 1) / 2;
+}
+
+extern "C" int64_t mixer_vis_elems(int32_t nant, int32_t nch) {
+    if (nant <= 0 || nch <= 0) return 0;
+    return (int64_t)nch * mixer_vis_tiles(nant) * 2 * 128 * 128;
+}
+
+extern "C" int mixer_xcorr_tri(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt,
+                               int64_t kbeg, int64_t klen, int32_t mode, void* vis, int32_t* err,
+                               void* stream) {
+    if (!planes || !vis || nant <= 0 || nch <= 0 || kt <= 0 || kt % 16 != 0) return MIXER_EINVAL;
+    if (kbeg < 0 || kbeg % 16 != 0 || klen <= 0 || kbeg + klen > kt) return MIXER_EINVAL;
+    if (mode != MIXER_VIS_STORE_I32 && mode != MIXER_VIS_ACC_I32 && mode != MIXER_VIS_ACC_I64)
+        return MIXER_EINVAL;
+    if (kt > (int64_t)INT32_MAX || nant > 65536 || nch > 65536) return MIXER_EINVAL;
+    if (reinterpret_cast<uintptr_t>(planes) % 16 != 0) return MIXER_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (mode != MIXER_VIS_ACC_I64) {
+        if (klen > MIXER_KMAX_I32) return MIXER_EOVERFLOW;
+        return mixer::xcorr_launch(planes, nant, nch, kt, kbeg, klen, mode, vis, err, st);
+    }
+    for (int64_t k = 0; k < klen; k += MIXER_KMAX_I32) {
+        const int64_t len = (klen - k) < MIXER_KMAX_I32 ? (klen - k) : MIXER_KMAX_I32;
+        const int rc = mixer::xcorr_launch(planes, nant, nch, kt, kbeg + k, len, mode, vis, err, st);
+        if (rc != MIXER_OK) return rc;
+    }
+    return MIXER_OK;
+}

@@ -1,0 +1,308 @@
+"""Python binding of the B200 X-engine C-ABI (libmixer_b200.so, include/mixer.h).
+
+The library is the product; this module only loads it with ctypes and passes
+pointers through.  Device buffers are torch tensors (or raw integer device
+addresses); streams are torch.cuda.Stream objects or raw cudaStream_t ints.
+If the shared library is missing the import fails: there is no fallback.
+
+Entry points and the reference symbol each replaces:
+    corner_turn      k_packAB            src/rx_host_corr.cu:61-72
+    xcorr_tri        cgemm_blk_t<ACC>    src/cgemm.cuh:28-69
+    vis_flush        k_flush_cube        src/rx_host_corr.cu:90-95
+    vis_dump_f32     --dump record       src/rx_host_corr.cu:187,225-227
+    grid             k_grid_cube (+k_diff) src/rx_host_corr.cu:74-85
+    image_fft        cufftExecC2C + host fftshift src/rx_host_corr.cu:205-235
+    gen_packets      tx_host k_sky + DAQIRI capture src/tx_host.cu:41-79
+    ArrayContext     gpu_thread / publish loop src/rx_host_corr.cu:143-239
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmixer_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `make -C {_HERE}` (or __graft_entry__.build()); "
+        "the X-engine has no CPU fallback")
+_lib = C.CDLL(LIB_PATH)
+
+# ---- constants (include/mixer.h) ------------------------------------------
+OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, EOVERFLOW, ENODEV, EBUSY = 0, -1, -2, -3, -4, -5, -6, -7
+WIRE_NANT, WIRE_ACTIVE_NCH, WIRE_TPKT = 256, 128, 32
+WIRE_PAYLOAD_BYTES, WIRE_HDR_BYTES, WIRE_BYTES, WIRE_SEQ_BYTE, WIRE_PPB = 8192, 64, 8256, 48, 256
+WIRE_UDP_PORT = 4096
+KMAX_I32 = 65408
+VIS_STORE_I32, VIS_ACC_I32, VIS_ACC_I64 = 0, 1, 2
+
+
+class MixerError(RuntimeError):
+    def __init__(self, rc: int, what: str):
+        super().__init__(f"{what}: {_lib.mixer_strerror(rc).decode()} (status {rc})")
+        self.rc = rc
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != OK:
+        raise MixerError(rc, what)
+
+
+_vp, _i32, _i64, _u32, _u16, _u64, _f64 = (C.c_void_p, C.c_int32, C.c_int64, C.c_uint32,
+                                           C.c_uint16, C.c_uint64, C.c_double)
+
+
+class ArrayDesc(C.Structure):
+    _fields_ = [("nant", _i32), ("nch", _i32), ("tpkt", _i32), ("ksub", _i32),
+                ("nsub_dump", _i32), ("side_x", _i32), ("grid", _i32), ("pkt_stride", _i32),
+                ("hdr_bytes", _i32), ("max_heaps", _i32)]
+
+
+def _sig(name, res, *args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+_sig("mixer_strerror", C.c_char_p, C.c_int)
+_sig("mixer_device_ok", C.c_int)
+_sig("mixer_vis_tiles", _i32, _i32)
+_sig("mixer_vis_elems", _i64, _i32, _i32)
+_sig("mixer_corner_turn", C.c_int, _vp, _i64, _i32, _i32, _i32, _i32, _i32, _u32, _vp, _i64, _i64,
+     _vp, _vp, _vp)
+_sig("mixer_xcorr_tri", C.c_int, _vp, _i32, _i32, _i64, _i64, _i64, _i32, _vp, _vp, _vp)
+_sig("mixer_vis_flush", C.c_int, _vp, _vp, _i64, _vp)
+_sig("mixer_vis_dump_f32", C.c_int, _vp, _i32, _i32, _vp, _vp)
+_sig("mixer_vis_unpack_i64", C.c_int, _vp, _i32, _i32, _vp, _vp)
+_sig("mixer_grid", C.c_int, _vp, _i32, _i32, _i32, _i32, _vp, _vp, _vp)
+_sig("mixer_image_fft", C.c_int, _vp, _i32, _i32, _vp, _vp, _vp, _vp)
+_sig("mixer_sky_table", C.c_int, _i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp)
+_sig("mixer_gen_packets", C.c_int, _vp, _i64, _i32, _i32, _i32, _i32, _i32, _i64, _u32, _u16, _vp,
+     _f64, _u64, _i32, _vp)
+_sig("mixer_desc_default", C.c_int, C.POINTER(ArrayDesc))
+_sig("mixer_create", C.c_int, C.POINTER(ArrayDesc), C.POINTER(_vp))
+_sig("mixer_destroy", C.c_int, _vp)
+_sig("mixer_reset", C.c_int, _vp, _vp)
+_sig("mixer_correlate", C.c_int, _vp, _vp, _i64, _u32, _i32, _vp)
+_sig("mixer_correlate_i32", C.c_int, _vp, _vp, _i64, _u32, _i32, _vp)
+_sig("mixer_integrate", C.c_int, _vp, _vp)
+_sig("mixer_dump", C.c_int, _vp, _vp, _i32, _vp)
+_sig("mixer_dump_to_file", C.c_int, _vp, C.c_char_p, _vp)
+_sig("mixer_read_vis_i64", C.c_int, _vp, _vp, _i32, _i32, _vp)
+_sig("mixer_image", C.c_int, _vp, _vp, _vp, _vp, _i32, _i32, _vp)
+_sig("mixer_stats", C.c_int, _vp, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i32))
+_sig("mixer_state_ptr", _vp, _vp)
+_sig("mixer_shm_open", C.c_int, C.c_char_p, _i32, _i32, C.POINTER(_vp))
+_sig("mixer_shm_publish", C.c_int, _vp, _vp, _vp, _vp, _u64)
+_sig("mixer_shm_close", C.c_int, _vp, _i32)
+
+EXPORTED = [
+    "mixer_vis_tiles", "mixer_vis_elems", "mixer_strerror", "mixer_device_ok",
+    "mixer_corner_turn", "mixer_xcorr_tri", "mixer_vis_flush", "mixer_vis_dump_f32",
+    "mixer_vis_unpack_i64", "mixer_grid", "mixer_image_fft", "mixer_sky_table",
+    "mixer_gen_packets", "mixer_desc_default", "mixer_create", "mixer_destroy", "mixer_reset",
+    "mixer_correlate", "mixer_correlate_i32", "mixer_integrate", "mixer_dump",
+    "mixer_dump_to_file", "mixer_read_vis_i64", "mixer_image", "mixer_stats", "mixer_state_ptr",
+    "mixer_shm_open", "mixer_shm_publish", "mixer_shm_close",
+]
+
+
+def lib():
+    return _lib
+
+
+def _ptr(x) -> int | None:
+    """Device / host address of a torch tensor, numpy array or raw int (None -> NULL)."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if hasattr(x, "ctypes"):
+        return x.ctypes.data
+    raise TypeError(f"cannot take the address of {type(x)}")
+
+
+def _stream(s) -> int | None:
+    if s is None:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return torch.cuda.current_stream().cuda_stream
+        except ImportError:
+            pass
+        return None
+    if isinstance(s, int):
+        return s
+    return s.cuda_stream
+
+
+def vis_tiles(nant: int) -> int:
+    return _lib.mixer_vis_tiles(nant)
+
+
+def vis_elems(nant: int, nch: int) -> int:
+    return _lib.mixer_vis_elems(nant, nch)
+
+
+def device_ok() -> bool:
+    return _lib.mixer_device_ok() == OK
+
+
+# ---- stateless entry points ------------------------------------------------
+
+def corner_turn(packets, pkt_stride, hdr_bytes, nant, nch, tpkt, nheaps, seq0, planes, kt, k0=0,
+                seq_errors=None, err=None, stream=None):
+    _check(_lib.mixer_corner_turn(_ptr(packets), pkt_stride, hdr_bytes, nant, nch, tpkt, nheaps,
+                                  seq0 & 0xFFFFFFFF, _ptr(planes), kt, k0, _ptr(seq_errors),
+                                  _ptr(err), _stream(stream)), "mixer_corner_turn")
+
+
+def xcorr_tri(planes, nant, nch, kt, kbeg, klen, mode, vis, err=None, stream=None):
+    _check(_lib.mixer_xcorr_tri(_ptr(planes), nant, nch, kt, kbeg, klen, mode, _ptr(vis), _ptr(err),
+                                _stream(stream)), "mixer_xcorr_tri")
+
+
+def vis_flush(vis32, vis64, n, stream=None):
+    _check(_lib.mixer_vis_flush(_ptr(vis32), _ptr(vis64), n, _stream(stream)), "mixer_vis_flush")
+
+
+def vis_dump_f32(vis64, nant, nch, cube, stream=None):
+    _check(_lib.mixer_vis_dump_f32(_ptr(vis64), nant, nch, _ptr(cube), _stream(stream)),
+           "mixer_vis_dump_f32")
+
+
+def vis_unpack_i64(vis64, nant, nch, cube, stream=None):
+    _check(_lib.mixer_vis_unpack_i64(_ptr(vis64), nant, nch, _ptr(cube), _stream(stream)),
+           "mixer_vis_unpack_i64")
+
+
+def grid(vis64, nant, nch, side_x, G, out, prev=None, stream=None):
+    _check(_lib.mixer_grid(_ptr(vis64), nant, nch, side_x, G, _ptr(out), _ptr(prev),
+                           _stream(stream)), "mixer_grid")
+
+
+def image_fft(grid_i64, nch, G, img, vmax=None, vmin=None, stream=None):
+    _check(_lib.mixer_image_fft(_ptr(grid_i64), nch, G, _ptr(img), _ptr(vmax), _ptr(vmin),
+                                _stream(stream)), "mixer_image_fft")
+
+
+def sky_table(nant, nch, side_x, sources):
+    """sources: list of (l, m, amp0, amp1).  Returns numpy float64 [nch][nant][2]."""
+    import numpy as np
+    n = len(sources)
+    arr = np.asarray(sources, dtype=np.float64).reshape(n, 4) if n else np.zeros((0, 4))
+    l, m, a0, a1 = (np.ascontiguousarray(arr[:, q]) for q in range(4))
+    out = np.zeros((nch, nant, 2), dtype=np.float64)
+    _check(_lib.mixer_sky_table(nant, nch, side_x, n, _ptr(l), _ptr(m), _ptr(a0), _ptr(a1),
+                                _ptr(out)), "mixer_sky_table")
+    return out
+
+
+def gen_packets(packets, pkt_stride, hdr_bytes, nant, nch, tpkt, nheaps, heap0, seq0, udp_port,
+                sky, sigma, seed, noise_mode=0, stream=None):
+    _check(_lib.mixer_gen_packets(_ptr(packets), pkt_stride, hdr_bytes, nant, nch, tpkt, nheaps,
+                                  heap0, seq0 & 0xFFFFFFFF, udp_port, _ptr(sky), float(sigma),
+                                  seed & 0xFFFFFFFFFFFFFFFF, noise_mode, _stream(stream)),
+           "mixer_gen_packets")
+
+
+# ---- array context ------------------------------------------------------------
+
+def default_desc() -> ArrayDesc:
+    d = ArrayDesc()
+    _check(_lib.mixer_desc_default(C.byref(d)), "mixer_desc_default")
+    return d
+
+
+class ArrayContext:
+    """One array's resident X-engine state (int64 cube, staging, imaging)."""
+
+    def __init__(self, desc: ArrayDesc | None = None, **kw):
+        d = desc if desc is not None else default_desc()
+        for k, v in kw.items():
+            setattr(d, k, v)
+        self.desc = d
+        h = _vp()
+        _check(_lib.mixer_create(C.byref(d), C.byref(h)), "mixer_create")
+        self._h = h.value
+
+    def close(self):
+        if self._h:
+            _lib.mixer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def reset(self, stream=None):
+        _check(_lib.mixer_reset(self._h, _stream(stream)), "mixer_reset")
+
+    def correlate(self, packets, nheaps, seq0=0, on_device=True, stream=None):
+        _check(_lib.mixer_correlate(self._h, _ptr(packets), nheaps, seq0 & 0xFFFFFFFF,
+                                    1 if on_device else 0, _stream(stream)), "mixer_correlate")
+
+    def correlate_i32(self, packets, nheaps, seq0=0, on_device=True, stream=None):
+        _check(_lib.mixer_correlate_i32(self._h, _ptr(packets), nheaps, seq0 & 0xFFFFFFFF,
+                                        1 if on_device else 0, _stream(stream)),
+               "mixer_correlate_i32")
+
+    def integrate(self, stream=None):
+        _check(_lib.mixer_integrate(self._h, _stream(stream)), "mixer_integrate")
+
+    def dump(self, out, on_device=True, stream=None):
+        _check(_lib.mixer_dump(self._h, _ptr(out), 1 if on_device else 0, _stream(stream)),
+               "mixer_dump")
+
+    def dump_to_file(self, path: str, stream=None):
+        _check(_lib.mixer_dump_to_file(self._h, path.encode(), _stream(stream)),
+               "mixer_dump_to_file")
+
+    def read_vis_i64(self, out, full_square=True, on_device=True, stream=None):
+        _check(_lib.mixer_read_vis_i64(self._h, _ptr(out), 1 if full_square else 0,
+                                       1 if on_device else 0, _stream(stream)),
+               "mixer_read_vis_i64")
+
+    def image(self, img, vmax=None, vmin=None, delta=False, on_device=True, stream=None):
+        _check(_lib.mixer_image(self._h, _ptr(img), _ptr(vmax), _ptr(vmin), 1 if delta else 0,
+                                1 if on_device else 0, _stream(stream)), "mixer_image")
+
+    def stats(self):
+        s, e, k = _i64(), _i64(), _i32()
+        rc = _lib.mixer_stats(self._h, C.byref(s), C.byref(e), C.byref(k))
+        if rc not in (OK, ETIMEOUT):
+            _check(rc, "mixer_stats")
+        return {"samples": s.value, "seq_errors": e.value, "kernel_err": k.value}
+
+    def state_ptr(self) -> int:
+        return _lib.mixer_state_ptr(self._h)
+
+
+class Corr32Shm:
+    """Corr32 image publisher (src/rx_host_corr.cu:97-105)."""
+
+    def __init__(self, name: str, nch: int, G: int):
+        h = _vp()
+        _check(_lib.mixer_shm_open(name.encode(), nch, G, C.byref(h)), "mixer_shm_open")
+        self._h = h.value
+
+    def publish(self, img, vmax, vmin, write_seq: int):
+        _check(_lib.mixer_shm_publish(self._h, _ptr(img), _ptr(vmax), _ptr(vmin), write_seq),
+               "mixer_shm_publish")
+
+    def close(self, unlink=True):
+        if self._h:
+            _lib.mixer_shm_close(self._h, 1 if unlink else 0)
+            self._h = None
