@@ -37,6 +37,20 @@ HEAPS_PER_SUB = KSUB // TPKT                   # 64
 SIGMA, SEED = 8.0, 20261203
 METRIC = "int8 cGEMM TOPS & input Gb/s vs roofline (stream vs plain); p50/p99 dump latency"
 L2_BYTES = 126 * 1024 * 1024
+# DRAM bytes of one k_xcorr_tri launch over its algorithmic bytes (planes read
+# once + int64 cube read and written), from the ncu capture of the N 1024,
+# C 64, K 4096 case: 1.6957 GB measured / 1.7456 GB algorithmic.
+XCORR_TRAFFIC_RATIO = 1.6957 / 1.7456
+
+
+def configure(nch):
+    """Channel count of the packets; the payload stays 8192 bytes (2 x nch x tpkt)."""
+    global NCH, TPKT, STRIDE, HEAPS_PER_SUB
+    if 4096 % nch or (4096 // nch) % 16:
+        raise SystemExit("--nch must divide 4096 with 4096/nch a multiple of 16")
+    NCH, TPKT = nch, 4096 // nch
+    STRIDE = HDR + 2 * NCH * TPKT
+    HEAPS_PER_SUB = KSUB // TPKT
 
 
 def sources(seed=SEED):
@@ -239,6 +253,40 @@ def run_reference(args):
     return 0
 
 
+def run_sweep(args):
+    """Per-launch time of k_xcorr_tri against K (samples per launch) and epilogue
+    mode on device-resident random planes: separates per-tile overhead from the
+    steady-state tensor rate.  One JSON line per point."""
+    import torch
+    import mixer
+    dev = torch.device("cuda:0")
+    for (N, C) in [(1024, 64), (4096, 8), (256, 128)]:
+        n = mixer.vis_elems(N, C)
+        v64 = torch.zeros(n, dtype=torch.int64, device=dev)
+        v32 = torch.zeros(n, dtype=torch.int32, device=dev)
+        for K in [1024, 2048, 4096, 8192, 16384, 32768]:
+            planes = torch.randint(-128, 128, (2 * C * N * K,), dtype=torch.int8, device=dev)
+            for mode, vis in [(mixer.VIS_STORE_I32, v32), (mixer.VIS_ACC_I64, v64)]:
+                for _ in range(2):
+                    mixer.xcorr_tri(planes, N, C, K, 0, K, mode, vis)
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(5):
+                    mixer.xcorr_tri(planes, N, C, K, 0, K, mode, vis)
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / 5
+                nb = (N + 127) // 128
+                tiles = C * nb * (nb + 1) // 2
+                print(json.dumps({"N": N, "C": C, "K": K, "mode": mode, "ms": ms,
+                                  "tri_tops": 8.0 * N * (N + 1) / 2 * K * C / ms / 1e9,
+                                  "tile_tops": 8.0 * tiles * 128 * 128 * K / ms / 1e9}), flush=True)
+            del planes
+    return 0
+
+
 def run_ours(args):
     import torch
     import mixer
@@ -293,6 +341,14 @@ def run_ours(args):
     packets_all = sum_over_ranks(pg, float(npk * args.steps), dev)
     value = wire_gbps(packets_all, t_max)
     tops = tri_ops(kt) * args.steps * world / t_max / 1e12
+
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile_case": True, "nch": NCH, "subints": S,
+                              "ms_per_step": ms_total / args.steps,
+                              "xcorr_ms": statistics.mean(gemm_ms),
+                              "corner_turn_ms": statistics.mean(ct_ms)}))
+        return 0
 
     # ---- plain form: one launch pair per sub-integration ------------------------
     plain_steps = max(1, min(args.steps, 5))
@@ -355,12 +411,16 @@ def run_ours(args):
 
     # ---- roofline of the dominant kernel (the GEMM) --------------------------------
     peaks = measured_peaks()
-    bf16 = peaks.get("bf16_tflops")
+    sustained = ms_total > 500.0          # a long timed region runs under the power cap
+    bf16 = peaks.get("bf16_tflops_sustained" if sustained else "bf16_tflops")
+    kind = "sustained" if sustained else "burst"
     if bf16:
-        peak, peak_src = 2.0 * bf16, "2 x measured cuBLAS bf16 burst (MEASURED_PEAKS.json); " \
-                                     "B200 dense int8 = 2 x dense bf16"
+        peak = 2.0 * bf16
+        peak_src = (f"of measured: 2 x cuBLAS bf16 {kind} ({bf16} TF/s, MEASURED_PEAKS.json); "
+                    "B200 dense int8 rate = 2 x dense bf16 rate")
     else:
-        peak, peak_src = 2.0 * 1590.0, "2 x fallback bf16 1.59 PF/s"
+        peak = 2.0 * (1400.0 if sustained else 1590.0)
+        peak_src = f"of fallback: 2 x bf16 {kind}"
     gemm_avg = statistics.mean(gemm_ms) / 1e3
     achieved = tri_ops(kt) / gemm_avg / 1e12
     ct_avg = statistics.mean(ct_ms) / 1e3
@@ -389,7 +449,9 @@ def run_ours(args):
                     "xcorr_ms": 1e3 * gemm_avg},
         "roofline": {"kernel": "k_xcorr_tri", "bound": "tensor", "achieved": achieved,
                      "peak": peak, "unit": "TOPS", "frac": achieved / peak,
-                     "peak_source": peak_src, "traffic": None,
+                     "peak_source": peak_src,
+                     "traffic": XCORR_TRAFFIC_RATIO * (2 * NCH * NANT * kt + 2 * 8 * mixer.vis_elems(NANT, NCH)),
+                     "traffic_note": "bytes per launch, scaled from the ncu capture of a smaller case",
                      "ops_per_launch": tri_ops(kt)},
         "clocks": clk.summary(),
         "gpu_launches": 2 * args.steps,
@@ -410,7 +472,7 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=8, help="sub-integrations per step")
@@ -419,11 +481,19 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-channels", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nch", type=int, default=256, help="channels per packet (tpkt = 4096/nch)")
+    ap.add_argument("--sweep-xcorr", action="store_true",
+                    help="time the GEMM kernel over K and epilogue mode (JSON lines)")
+    ap.add_argument("--profile", action="store_true",
+                    help="device-resident steps only (small case for ncu captures)")
     args = ap.parse_args()
-    if args.warmup < 3 and args.impl == "ours":
+    configure(args.nch)
+    if args.warmup < 3 and args.impl == "ours" and not args.profile:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "reference":
         return run_reference(args)
+    if args.sweep_xcorr:
+        return run_sweep(args)
     return run_ours(args)
 
 
