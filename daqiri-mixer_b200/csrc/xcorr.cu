@@ -4,20 +4,23 @@
 // Replaces cgemm_blk_t<ACC> (reference src/cgemm.cuh:28-69).  The reference
 // issues four wmma 16x16x16 products per tile from global memory, negates the
 // A_im fragment (src/cgemm.cuh:52, wraps for -128) and computes the full
-// square.  Here, per channel c and 128 x 128 tile (i, j) with j <= i:
+// square.  Here, per channel c and 128 x 128 tile (i, j) with j <= i, the B
+// operand is the 256-row stack [Xr_j ; Xi_j] (the two plane tiles sit next to
+// each other in shared memory), so two M=128, N=256 MMAs per 32-sample step
+// produce all four real products:
 //
-//   acc_re += Xr_i Xr_j^T + Xi_i Xi_j^T          (TMEM columns   0..127)
-//   acc_p1 += Xi_i Xr_j^T                        (TMEM columns 128..255)
-//   acc_p2 += Xr_i Xi_j^T                        (TMEM columns 256..383)
-//   Re V = acc_re,  Im V = acc_p1 - acc_p2       (epilogue)
+//   D1 = Xr_i [Xr_j ; Xi_j]^T = [ R1 | P2 ]      (TMEM columns   0..255)
+//   D2 = Xi_i [Xr_j ; Xi_j]^T = [ P1 | R2 ]      (TMEM columns 256..511)
+//   Re V = R1 + R2,  Im V = P1 - P2              (epilogue)
 //
-// so no operand is ever negated and every int8 input, -128 included, is exact.
-// Operands come from the corner-turned planes [2][C][N][kt] through 4-D TMA
-// tensor loads (128-byte swizzle, 128 x 128-byte boxes), staged in a 3-deep
-// shared-memory ring.  One elected thread issues all tcgen05.mma; int32
-// accumulators live in TMEM for the whole K range of the launch; four
-// epilogue warps read them back with tcgen05.ld and add them into the
-// tile-packed int32 or int64 cube in HBM.
+// No operand is ever negated, so every int8 input, -128 included, is exact.
+// Diagonal tiles (i == j) use the A tiles [Xr_i ; Xi_i] as B and load half
+// the bytes.  Operands come from the corner-turned planes [2][C][N][kt]
+// through 4-D TMA tensor loads (128-byte swizzle, 128 x 128-byte boxes)
+// into a 3-deep shared-memory ring.  One elected thread issues all
+// tcgen05.mma; the int32 accumulators stay in TMEM for the whole K range of
+// the launch; four epilogue warps read them back with tcgen05.ld and add
+// them into the tile-packed int32 or int64 cube in HBM.
 //
 // Warp roles (192 threads, one CTA per SM, persistent over work items):
 //   warp 0      TMA producer
@@ -36,8 +39,8 @@ constexpr int kTileBytes = kTile * kKc;          // 16 KiB
 constexpr int kStageBytes = 4 * kTileBytes;      // Ar, Ai, Br, Bi
 constexpr int kBarBytes = 256;
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 + kBarBytes;
-constexpr uint32_t kTmemCols = 512;              // 3 x 128 used
-constexpr uint32_t kIdesc = idesc_i8(128, 128);
+constexpr uint32_t kTmemCols = 512;              // D1 (256) + D2 (256)
+constexpr uint32_t kIdesc = idesc_i8(128, 256);
 
 struct XcorrArgs {
     int32_t nant, nch, nblk, ntiles;
@@ -57,27 +60,34 @@ __device__ __forceinline__ void decode_tile(int t, int& i, int& j) {
     j = t - ii * (ii + 1) / 2;
 }
 
-// Three 32x32b.x16 TMEM loads (re, p1, p2 columns) and the wait, in one asm
-// statement so no use of the results can be scheduled before the wait.
-__device__ __forceinline__ void tmem_ld3_x16(uint32_t a0, uint32_t a1, uint32_t a2,
-                                             uint32_t (&r)[16], uint32_t (&p)[16],
-                                             uint32_t (&q)[16]) {
+// Four 32x32b.x16 TMEM loads and the wait, in one asm statement so no use of
+// the results can be scheduled before the wait.
+__device__ __forceinline__ void tmem_ld4_x16(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                             uint32_t (&r)[4][16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%48];\n\t"
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%64];\n\t"
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%49];\n\t"
+        "{%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%65];\n\t"
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47}, [%50];\n\t"
+        "{%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47}, [%66];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%67];\n\t"
         "tcgen05.wait::ld.sync.aligned;"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-          "=r"(r[14]), "=r"(r[15]), "=r"(p[0]), "=r"(p[1]), "=r"(p[2]), "=r"(p[3]), "=r"(p[4]),
-          "=r"(p[5]), "=r"(p[6]), "=r"(p[7]), "=r"(p[8]), "=r"(p[9]), "=r"(p[10]), "=r"(p[11]),
-          "=r"(p[12]), "=r"(p[13]), "=r"(p[14]), "=r"(p[15]), "=r"(q[0]), "=r"(q[1]), "=r"(q[2]),
-          "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7]), "=r"(q[8]), "=r"(q[9]),
-          "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]), "=r"(q[15])
-        : "r"(a0), "r"(a1), "r"(a2)
+        : "=r"(r[0][0]), "=r"(r[0][1]), "=r"(r[0][2]), "=r"(r[0][3]), "=r"(r[0][4]),
+          "=r"(r[0][5]), "=r"(r[0][6]), "=r"(r[0][7]), "=r"(r[0][8]), "=r"(r[0][9]),
+          "=r"(r[0][10]), "=r"(r[0][11]), "=r"(r[0][12]), "=r"(r[0][13]), "=r"(r[0][14]),
+          "=r"(r[0][15]), "=r"(r[1][0]), "=r"(r[1][1]), "=r"(r[1][2]), "=r"(r[1][3]),
+          "=r"(r[1][4]), "=r"(r[1][5]), "=r"(r[1][6]), "=r"(r[1][7]), "=r"(r[1][8]),
+          "=r"(r[1][9]), "=r"(r[1][10]), "=r"(r[1][11]), "=r"(r[1][12]), "=r"(r[1][13]),
+          "=r"(r[1][14]), "=r"(r[1][15]), "=r"(r[2][0]), "=r"(r[2][1]), "=r"(r[2][2]),
+          "=r"(r[2][3]), "=r"(r[2][4]), "=r"(r[2][5]), "=r"(r[2][6]), "=r"(r[2][7]),
+          "=r"(r[2][8]), "=r"(r[2][9]), "=r"(r[2][10]), "=r"(r[2][11]), "=r"(r[2][12]),
+          "=r"(r[2][13]), "=r"(r[2][14]), "=r"(r[2][15]), "=r"(r[3][0]), "=r"(r[3][1]),
+          "=r"(r[3][2]), "=r"(r[3][3]), "=r"(r[3][4]), "=r"(r[3][5]), "=r"(r[3][6]),
+          "=r"(r[3][7]), "=r"(r[3][8]), "=r"(r[3][9]), "=r"(r[3][10]), "=r"(r[3][11]),
+          "=r"(r[3][12]), "=r"(r[3][13]), "=r"(r[3][14]), "=r"(r[3][15])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3)
         : "memory");
 }
 
@@ -168,7 +178,7 @@ __global__ void __launch_bounds__(192, 1)
             int stage = 0;
             uint32_t phase = 0, acc_phase = 0;
             bool ok = true;
-            const uint32_t t_re = tmem, t_p1 = tmem + 128, t_p2 = tmem + 256;
+            const uint32_t t_d1 = tmem, t_d2 = tmem + 256;
             for (int64_t w = blockIdx.x; w < args.nwork; w += gridDim.x) {
                 const int c = (int)(w / args.ntiles);
                 const int t = (int)(w - (int64_t)c * args.ntiles);
@@ -189,16 +199,14 @@ __global__ void __launch_bounds__(192, 1)
                     const uint32_t sb = base + stage * kStageBytes;
                     const uint64_t ar = sdesc_sw128(sb);
                     const uint64_t ai = sdesc_sw128(sb + kTileBytes);
-                    const uint64_t br = diag ? ar : sdesc_sw128(sb + 2 * kTileBytes);
-                    const uint64_t bi = diag ? ai : sdesc_sw128(sb + 3 * kTileBytes);
+                    // 256-row B operand [Xr_j ; Xi_j]: two adjacent 16 KiB tiles
+                    const uint64_t b = diag ? ar : sdesc_sw128(sb + 2 * kTileBytes);
 #pragma unroll
                     for (int kk = 0; kk < kKc / 32; ++kk) {
                         const uint64_t o = (uint64_t)((kk * 32) >> 4);   // 32-byte K step
                         const uint32_t acc = (kc > 0 || kk > 0) ? 1u : 0u;
-                        mma_i8(t_re, ar + o, br + o, kIdesc, acc);
-                        mma_i8(t_re, ai + o, bi + o, kIdesc, 1u);
-                        mma_i8(t_p1, ai + o, br + o, kIdesc, acc);
-                        mma_i8(t_p2, ar + o, bi + o, kIdesc, acc);
+                        mma_i8(t_d1, ar + o, b + o, kIdesc, acc);
+                        mma_i8(t_d2, ai + o, b + o, kIdesc, acc);
                     }
                     tc_commit(bar(EMPTY + stage));   // stage free once these MMAs finish
                     if (++stage == kStages) {
@@ -236,8 +244,8 @@ __global__ void __launch_bounds__(192, 1)
             const size_t tb = ((size_t)c * args.ntiles + t) * (size_t)(2 * kTile * kTile);
 #pragma unroll 1
             for (int n0 = 0; n0 < kTile; n0 += 16) {
-                uint32_t re[16], p1[16], p2[16];
-                tmem_ld3_x16(trow + n0, trow + 128 + n0, trow + 256 + n0, re, p1, p2);
+                uint32_t r[4][16];   // R1, P2, P1, R2
+                tmem_ld4_x16(trow + n0, trow + 128 + n0, trow + 256 + n0, trow + 384 + n0, r);
                 if (n0 == kTile - 16) {              // all of this tile's TMEM is read
                     tc_fence_before();
                     mbar_arrive(bar(ACCE));
@@ -247,8 +255,8 @@ __global__ void __launch_bounds__(192, 1)
                     unsigned long long* v = reinterpret_cast<unsigned long long*>(args.vis);
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
-                        const int32_t vr = (int32_t)re[e];
-                        const int32_t vi = (int32_t)(p1[e] - p2[e]);
+                        const int32_t vr = (int32_t)(r[0][e] + r[3][e]);
+                        const int32_t vi = (int32_t)(r[2][e] - r[1][e]);
                         atomicAdd(v + e0 + (size_t)e * kTile, (unsigned long long)(long long)vr);
                         atomicAdd(v + e0 + (size_t)e * kTile + kTile * kTile,
                                   (unsigned long long)(long long)vi);
@@ -257,16 +265,16 @@ __global__ void __launch_bounds__(192, 1)
                     int* v = reinterpret_cast<int*>(args.vis);
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
-                        atomicAdd(v + e0 + (size_t)e * kTile, (int)re[e]);
+                        atomicAdd(v + e0 + (size_t)e * kTile, (int)(r[0][e] + r[3][e]));
                         atomicAdd(v + e0 + (size_t)e * kTile + kTile * kTile,
-                                  (int)(p1[e] - p2[e]));
+                                  (int)(r[2][e] - r[1][e]));
                     }
                 } else {
                     int* v = reinterpret_cast<int*>(args.vis);
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
-                        v[e0 + (size_t)e * kTile] = (int)re[e];
-                        v[e0 + (size_t)e * kTile + kTile * kTile] = (int)(p1[e] - p2[e]);
+                        v[e0 + (size_t)e * kTile] = (int)(r[0][e] + r[3][e]);
+                        v[e0 + (size_t)e * kTile + kTile * kTile] = (int)(r[2][e] - r[1][e]);
                     }
                 }
             }
