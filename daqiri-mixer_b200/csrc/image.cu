@@ -16,6 +16,7 @@
 // order, runs radix-2 butterflies along rows then columns in shared memory
 // with twiddles generated in FP64, and writes Re(F) shifted by G/2 in both
 // axes together with the channel's max and min.
+#include <mutex>
 #include "common.cuh"
 
 namespace mixer {
@@ -232,4 +233,44 @@ extern "C" int mixer_image_fft(const int64_t* grid, int32_t nch, int32_t G, floa
         reinterpret_cast<const long long*>(grid), G, logG, img, vmax, vmin);
     MIXER_CK(cudaGetLastError());
     return MIXER_OK;
+}
+
+// ---- imaging without allocation ---------------------------------------------
+// The grid scratch of mixer_image_noalloc: a fixed array in the library's
+// device image (re, im int64 per cell), shared by every call on a device.
+namespace mixer {
+namespace {
+__device__ __align__(256) long long g_noalloc_grid[2 * (size_t)MIXER_NOALLOC_MAX_CELLS];
+
+// Device address of g_noalloc_grid on the current device, looked up once per
+// device with that device current.
+int noalloc_grid_address(int64_t** out) {
+    static std::mutex mu;
+    static int64_t* addr[64] = {};
+    int dev = 0;
+    MIXER_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return MIXER_EINVAL;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        MIXER_CK(cudaGetSymbolAddress(&p, g_noalloc_grid));
+        addr[dev] = static_cast<int64_t*>(p);
+    }
+    *out = addr[dev];
+    return MIXER_OK;
+}
+}  // namespace
+}  // namespace mixer
+
+extern "C" int mixer_image_noalloc(const int64_t* vis64, int32_t nant, int32_t nch, int32_t side_x,
+                                   int32_t G, float* img, float* vmax, float* vmin, void* stream) {
+    if (!vis64 || !img || nant <= 0 || nch <= 0 || side_x <= 0 || G <= 0) return MIXER_EINVAL;
+    if ((int64_t)nch * G * G > MIXER_NOALLOC_MAX_CELLS) return MIXER_EINVAL;
+    int64_t* grid = nullptr;
+    int rc = mixer::noalloc_grid_address(&grid);
+    if (rc != MIXER_OK) return rc;
+    // mixer_grid clears the cells it uses on `stream` before adding into them.
+    rc = mixer_grid(vis64, nant, nch, side_x, G, grid, nullptr, stream);
+    if (rc != MIXER_OK) return rc;
+    return mixer_image_fft(grid, nch, G, img, vmax, vmin, stream);
 }

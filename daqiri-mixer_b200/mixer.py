@@ -35,6 +35,7 @@ WIRE_NANT, WIRE_ACTIVE_NCH, WIRE_TPKT = 256, 128, 32
 WIRE_PAYLOAD_BYTES, WIRE_HDR_BYTES, WIRE_BYTES, WIRE_SEQ_BYTE, WIRE_PPB = 8192, 64, 8256, 48, 256
 WIRE_UDP_PORT = 4096
 KMAX_I32 = 65408
+NOALLOC_MAX_CELLS = 1 << 20
 VIS_STORE_I32, VIS_ACC_I32, VIS_ACC_I64 = 0, 1, 2
 
 
@@ -78,6 +79,7 @@ _sig("mixer_vis_dump_f32", C.c_int, _vp, _i32, _i32, _vp, _vp)
 _sig("mixer_vis_unpack_i64", C.c_int, _vp, _i32, _i32, _vp, _vp)
 _sig("mixer_grid", C.c_int, _vp, _i32, _i32, _i32, _i32, _vp, _vp, _vp)
 _sig("mixer_image_fft", C.c_int, _vp, _i32, _i32, _vp, _vp, _vp, _vp)
+_sig("mixer_image_noalloc", C.c_int, _vp, _i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp)
 _sig("mixer_sky_table", C.c_int, _i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp)
 _sig("mixer_gen_packets", C.c_int, _vp, _i64, _i32, _i32, _i32, _i32, _i32, _i64, _u32, _u16, _vp,
      _f64, _u64, _i32, _vp)
@@ -101,7 +103,8 @@ _sig("mixer_shm_close", C.c_int, _vp, _i32)
 EXPORTED = [
     "mixer_vis_tiles", "mixer_vis_elems", "mixer_strerror", "mixer_device_ok",
     "mixer_corner_turn", "mixer_xcorr_tri", "mixer_vis_flush", "mixer_vis_dump_f32",
-    "mixer_vis_unpack_i64", "mixer_grid", "mixer_image_fft", "mixer_sky_table",
+    "mixer_vis_unpack_i64", "mixer_grid", "mixer_image_fft", "mixer_image_noalloc",
+    "mixer_sky_table",
     "mixer_gen_packets", "mixer_desc_default", "mixer_create", "mixer_destroy", "mixer_reset",
     "mixer_correlate", "mixer_correlate_i32", "mixer_integrate", "mixer_dump",
     "mixer_dump_to_file", "mixer_read_vis_i64", "mixer_image", "mixer_stats", "mixer_state_ptr",
@@ -188,6 +191,13 @@ def grid(vis64, nant, nch, side_x, G, out, prev=None, stream=None):
 def image_fft(grid_i64, nch, G, img, vmax=None, vmin=None, stream=None):
     _check(_lib.mixer_image_fft(_ptr(grid_i64), nch, G, _ptr(img), _ptr(vmax), _ptr(vmin),
                                 _stream(stream)), "mixer_image_fft")
+
+
+def image_noalloc(vis64, nant, nch, side_x, G, img, vmax=None, vmin=None, stream=None):
+    """Grid + FFT image with the grid in the library's fixed device array (no
+    allocation); nch * G * G <= NOALLOC_MAX_CELLS.  See include/mixer.h."""
+    _check(_lib.mixer_image_noalloc(_ptr(vis64), nant, nch, side_x, G, _ptr(img), _ptr(vmax),
+                                    _ptr(vmin), _stream(stream)), "mixer_image_noalloc")
 
 
 def sky_table(nant, nch, side_x, sources):

@@ -138,6 +138,30 @@ int mixer_grid(const int64_t* vis64, int32_t nant, int32_t nch, int32_t side_x,
 int mixer_image_fft(const int64_t* grid, int32_t nch, int32_t G, float* img,
                     float* vmax, float* vmin, void* stream);
 
+/* Imaging without any device allocation: the same gridding + FFT as
+ * mixer_grid followed by mixer_image_fft, but the intermediate int64 grid
+ * lives in a fixed array inside the library instead of a caller or context
+ * buffer.  It has no counterpart in the reference.  It exists for callers
+ * that must not allocate device memory once they are running: a capture
+ * framework that hands out a fixed memory budget at start-up, a real-time
+ * receive loop where cudaMalloc / cudaFree could stall or synchronise the
+ * device, or a host whose allocator belongs to another runtime.
+ *   - Capacity: nch * G * G <= MIXER_NOALLOC_MAX_CELLS (16 MiB of int64 re/im
+ *     cells, e.g. 256 x 64 x 64 or 64 x 128 x 128); larger requests return
+ *     MIXER_EINVAL and touch nothing.
+ *   - The array is part of the library's device image, so every GPU that
+ *     loads the library holds those 16 MiB until the process exits.
+ *   - The first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - All calls share the one array and it keeps the previous call's
+ *     contents; each call clears it on `stream` before gridding.  Calls whose
+ *     work overlaps on the GPU (different streams, or several host threads)
+ *     race on the array and must be serialised by the caller.
+ * vis64 / img / vmax / vmin as for mixer_grid and mixer_image_fft. */
+#define MIXER_NOALLOC_MAX_CELLS (1 << 20)
+int mixer_image_noalloc(const int64_t* vis64, int32_t nant, int32_t nch, int32_t side_x,
+                        int32_t G, float* img, float* vmax, float* vmin, void* stream);
+
 /* ---- seeded packet source (replaces the DAQIRI capture / tx_host) -------- */
 
 /* Sky model of one source list, evaluated in FP64 on the host:
