@@ -287,6 +287,268 @@ def run_sweep(args):
     return 0
 
 
+def batched_arrays(seed=SEED + 2, small=False):
+    """48 independent arrays: N from {64, 96, ..., 1024}, C from {16, 32, ..., 512},
+    K from {256, 512, ..., 4096}, each with one point source plus sigma 12 noise.
+    small=True draws N from {64..256}, C from {16..64}: arrays too small to fill
+    the GPU in a launch of their own."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(48):
+        n = int(rng.choice(np.arange(64, (257 if small else 1025), 32)))
+        c = int(rng.choice(np.arange(16, (65 if small else 513), 16)))
+        k = int(rng.choice(np.arange(256, 4097, 256)))
+        l, m = rng.uniform(-0.4, 0.4, size=2)
+        out.append((n, c, k, float(l), float(m)))
+    return out
+
+
+def vis_checksum(torch, v):
+    w = torch.arange(v.numel(), dtype=torch.int64, device=v.device) * 2654435761 + 12345
+    return int((v.view(torch.int64) * w).sum().item())
+
+
+def run_batched(args):
+    """Config 'batched': uneven arrays, one persistent launch, autotuned, graph-replayed,
+    against one launch per array; per-array results compared by checksum."""
+    import torch
+    import mixer
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    arrays = batched_arrays(small=args.small_arrays)
+    probs, total_ops, in_bytes = [], 0.0, 0
+    for idx, (n, c, k, l, m) in enumerate(arrays):
+        tp = 16
+        stride = 64 + 2 * c * tp
+        nh = k // tp
+        sky = torch.from_numpy(mixer.sky_table(n, c, 32, [(l, m, 4.0, 0.0)])).to(dev)
+        pk = torch.empty(nh * n * stride, dtype=torch.uint8, device=dev)
+        mixer.gen_packets(pk, stride, 64, n, c, tp, nh, 0, 0, 4096 + idx, sky, 12.0, SEED + idx, 0)
+        planes = torch.empty(2 * c * n * k, dtype=torch.int8, device=dev)
+        mixer.corner_turn(pk, stride, 64, n, c, tp, nh, 0, planes, k, 0)
+        del pk, sky
+        vis = torch.zeros(mixer.vis_elems(n, c), dtype=torch.int64, device=dev)
+        probs.append({"planes": planes, "nant": n, "nch": c, "kt": k, "kbeg": 0, "klen": k,
+                      "mode": mixer.VIS_ACC_I64, "vis": vis})
+        total_ops += 8.0 * n * (n + 1) / 2 * k * c
+        in_bytes += 2 * n * k * c
+    torch.cuda.synchronize()
+    stream = torch.cuda.Stream()
+    reps = max(3, min(args.steps, 20))
+
+    def timed(fn):
+        with torch.cuda.stream(stream):
+            fn()
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+            stream.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def plain():
+        for p in probs:
+            mixer.xcorr_tri(p["planes"], p["nant"], p["nch"], p["kt"], 0, p["kt"],
+                            mixer.VIS_ACC_I64, p["vis"], stream=stream)
+
+    def zero():
+        with torch.cuda.stream(stream):     # same stream as the launches
+            for p in probs:
+                p["vis"].zero_()
+        stream.synchronize()
+
+    zero()
+    t_plain = timed(plain)
+    zero()
+    with torch.cuda.stream(stream):
+        plain()
+    stream.synchronize()
+    with torch.cuda.stream(stream):
+        sums_plain = [vis_checksum(torch, p["vis"]) for p in probs]
+    b = mixer.Batch(probs)
+    t_untuned = timed(lambda: b.run(stream))
+    t0 = time.perf_counter()
+    tuned_ms = b.autotune(reps=1, stream=stream)
+    tune_s = time.perf_counter() - t0
+    t_tuned = timed(lambda: b.run(stream))
+    b.capture_graph(stream)
+    t_graph = timed(lambda: b.replay(stream))
+    zero()
+    with torch.cuda.stream(stream):
+        b.replay(stream)
+    stream.synchronize()
+    with torch.cuda.stream(stream):
+        sums_batch = [vis_checksum(torch, p["vis"]) for p in probs]
+    info = b.info()
+    exact = sums_plain == sums_batch and info["kernel_err"] == 0
+    line = {
+        "metric": "batched uneven arrays: int8 cGEMM TOPS (triangle basis), batched vs plain",
+        "config": {"workload": ("48 small arrays, N in {64..256 step 32}, C in {16..64 step 16}"
+                                if args.small_arrays else
+                                "48 arrays, N in {64..1024 step 32}, C in {16..512 step 16}")
+                   + ", K in {256..4096 step 256}, 1 source + sigma 12 noise each (seeded)",
+                   "total_ops": total_ops, "plane_bytes": in_bytes},
+        "plain_ms": t_plain, "plain_tops": total_ops / t_plain / 1e9,
+        "batched_untuned_ms": t_untuned, "batched_tuned_ms": t_tuned, "graph_ms": t_graph,
+        "graph_tops": total_ops / t_graph / 1e9, "batched_over_plain": t_plain / t_graph,
+        "autotune_s": tune_s, "autotune_best_ms": tuned_ms,
+        "plan": {"nwork": info["nwork"], "order": ["lpt", "channel"][info["order"]],
+                 "split_per_class": {str(c): info["split"][c] for c in range(1, 9)}},
+        "bit_exact_vs_plain": exact, "reps": reps,
+    }
+    print(json.dumps(line))
+    b.close()
+    return 0 if exact else 1
+
+
+# Serving workload: (nant, nch, tpkt, ksub, nsub_dump, side) of the two stream types.
+SERVE_TYPES = {"256x128": (256, 128, 32, 256, 64, 16), "1024x64": (1024, 64, 64, 256, 64, 32)}
+
+
+def run_serve(args):
+    """Config 'serve': 8 concurrent streams (4 x 256 elements x 128 ch, 4 x 1024 x 64 ch)
+    of wire-format heaps from the seeded sky source, paced to an aggregate rate with
+    Poisson-jittered start / stop, admitted by a device-memory budget; dumps every 64
+    sub-integrations.  Reports sustained Gb/s and p50 / p99 dump latency; then an
+    unpaced run with all streams open gives the sustainable ceiling."""
+    import threading
+    import numpy as np
+    import torch
+    import mixer
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(SEED + 3)
+    kinds = ["256x128"] * 4 + ["1024x64"] * 4
+    pools = []
+    for i, kind in enumerate(kinds):
+        nant, nch, tpkt, ksub, nsub, side = SERVE_TYPES[kind]
+        hps = ksub // tpkt
+        stride = 64 + 2 * nch * tpkt
+        sky = torch.from_numpy(mixer.sky_table(
+            nant, nch, side, [(0.10, -0.05, 6.0, 0.0), (0.2, 0.0, 0.0, 1.5)])).to(dev)
+        pk = torch.empty(nsub * hps * nant * stride, dtype=torch.uint8, device=dev)
+        mixer.gen_packets(pk, stride, 64, nant, nch, tpkt, nsub * hps, 0, 0, 4096 + i, sky, 16.0,
+                          SEED + 100 + i, 0)
+        pools.append(pk)
+    torch.cuda.synchronize()
+
+    def one_run(run_s, gbps, budget, jitter):
+        srv = mixer.Server(budget_bytes=budget, max_streams=8, ring_subs=16, batch_subs=8)
+        per_stream = gbps / 8 * 1e9 / 8 if gbps > 0 else 0.0          # bytes / s
+        if jitter:
+            starts = np.cumsum(rng.exponential(run_s * 0.04, size=8))
+            stops = np.minimum(starts + rng.uniform(0.5, 0.9, size=8) * run_s, run_s)
+        else:
+            starts, stops = np.zeros(8), np.full(8, run_s)
+        t0 = time.perf_counter()
+        ids = [None] * 8
+        waits = [0.0] * 8
+        submitted = [0] * 8
+        active = [0.0] * 8
+        done = threading.Event()
+
+        def feeder(i):
+            kind = kinds[i]
+            nant, nch, tpkt, ksub, nsub, side = SERVE_TYPES[kind]
+            hps = ksub // tpkt
+            stride = 64 + 2 * nch * tpkt
+            sub_bytes = hps * nant * stride
+            d = mixer.make_desc(nant=nant, nch=nch, tpkt=tpkt, ksub=ksub, nsub_dump=nsub, side_x=side,
+                                grid=0, pkt_stride=stride, hdr_bytes=64, max_heaps=1)
+            while time.perf_counter() - t0 < starts[i]:
+                time.sleep(0.001)
+            tw = time.perf_counter()
+            while ids[i] is None and time.perf_counter() - t0 < stops[i]:
+                ids[i] = srv.try_open(d)
+                if ids[i] is None:
+                    time.sleep(0.002)
+            waits[i] = time.perf_counter() - tw
+            if ids[i] is None:
+                return
+            interval = sub_bytes / per_stream if per_stream > 0 else 0.0
+            nxt = time.perf_counter()
+            ta = nxt
+            j = 0
+            while time.perf_counter() - t0 < stops[i]:
+                if j % nsub == 0:                      # new lap over the pool: re-stamp seqs
+                    torch.cuda.synchronize()
+                    mixer.restamp_seq(pools[i], nsub * hps * nant, stride, j * hps * nant)
+                    torch.cuda.synchronize()
+                if interval > 0:
+                    while time.perf_counter() < nxt:
+                        time.sleep(min(0.0005, max(0.0, nxt - time.perf_counter())))
+                src = pools[i][(j % nsub) * sub_bytes:]
+                while not srv.submit(ids[i], src, hps, seq0=0):
+                    if time.perf_counter() - t0 >= stops[i]:
+                        break
+                    time.sleep(0.0002)
+                else:
+                    submitted[i] += sub_bytes
+                    j += 1
+                    nxt += interval
+                    continue
+                break
+            active[i] = time.perf_counter() - ta
+            # let the last full dump finish, then leave
+            time.sleep(0.05)
+            srv.close_stream(ids[i])
+            ids[i] = None
+
+        def poller():
+            while not done.is_set():
+                for sid in list(ids):
+                    if sid is not None:
+                        try:
+                            srv.poll(sid)
+                        except mixer.MixerError:
+                            pass
+                time.sleep(0.001)
+
+        th = [threading.Thread(target=feeder, args=(i,)) for i in range(8)]
+        pt = threading.Thread(target=poller)
+        pt.start()
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        wall = time.perf_counter() - t0
+        done.set()
+        pt.join()
+        st = srv.stats()
+        srv.close()
+        period = {k: v[4] * (v[3] // v[2]) * v[0] * (64 + 2 * v[1] * v[2]) / per_stream
+                  for k, v in SERVE_TYPES.items()} if per_stream > 0 else None
+        return {"wall_s": wall, "offered_gbps": gbps, "submitted_gbps": 8 * sum(submitted) / wall / 1e9,
+                "processed_gbps": 8 * st["bytes_processed"] / wall / 1e9,
+                "dumps": st["dumps"], "p50_dump_latency_ms": 1e3 * st["p50_latency_s"],
+                "p99_dump_latency_ms": 1e3 * st["p99_latency_s"],
+                "max_dump_latency_ms": 1e3 * st["max_latency_s"],
+                "integration_period_ms": ({k: 1e3 * v for k, v in period.items()} if period else None),
+                "per_stream_gbps": [round(8 * b / a / 1e9, 1) if a > 0 else 0.0
+                                    for b, a in zip(submitted, active)],
+                "per_stream_target_gbps": gbps / 8 if gbps > 0 else None,
+                "admitted": st["admitted"], "refused_attempts": st["refused"],
+                "streams_that_waited_for_admission": int(sum(w > 0.05 for w in waits)),
+                "admission_wait_s": [round(w, 3) for w in waits], "launches": st["launches"],
+                "work_items": st["work_items"], "seq_errors": st["seq_errors"],
+                "kernel_err": st["kernel_err"]}
+
+    paced = one_run(args.serve_seconds, args.serve_gbps, int(args.serve_budget_gb * (1 << 30)), True)
+    ceiling = one_run(min(args.serve_seconds, 6.0), 0.0, 64 << 30, False)
+    line = {"metric": "serving: sustained input Gb/s and p50/p99 dump latency",
+            "config": {"workload": "8 streams: 4 x (256 elements x 128 ch, tpkt 32), "
+                       "4 x (1024 elements x 64 ch, tpkt 64), K 256, 64 sub-integrations per dump, "
+                       "8256-byte heaps from the seeded sky source (device pools)",
+                       "paced_gbps": args.serve_gbps, "budget_gb": args.serve_budget_gb},
+            "paced": paced, "unpaced_ceiling": ceiling}
+    print(json.dumps(line))
+    ok = paced["kernel_err"] == 0 and ceiling["kernel_err"] == 0
+    return 0 if ok else 1
+
+
 def run_ours(args):
     import torch
     import mixer
@@ -482,6 +744,13 @@ def main():
     ap.add_argument("--ref-channels", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nch", type=int, default=256, help="channels per packet (tpkt = 4096/nch)")
+    ap.add_argument("--serve-seconds", type=float, default=20.0)
+    ap.add_argument("--serve-gbps", type=float, default=380.0)
+    ap.add_argument("--serve-budget-gb", type=float, default=6.0)
+    ap.add_argument("--config", default="plain", choices=["plain", "batched", "serve"],
+                    help="plain: the 1024-element array (headline); batched: 48 uneven arrays")
+    ap.add_argument("--small-arrays", action="store_true",
+                    help="batched config with arrays too small to fill the GPU alone")
     ap.add_argument("--sweep-xcorr", action="store_true",
                     help="time the GEMM kernel over K and epilogue mode (JSON lines)")
     ap.add_argument("--profile", action="store_true",
@@ -494,6 +763,10 @@ def main():
         return run_reference(args)
     if args.sweep_xcorr:
         return run_sweep(args)
+    if args.config == "batched":
+        return run_batched(args)
+    if args.config == "serve":
+        return run_serve(args)
     return run_ours(args)
 
 

@@ -1,0 +1,615 @@
+// server.cu -- streaming X-engine: concurrent array streams, continuous batching.
+//
+// The reference serves exactly one array from one NIC queue with one GPU
+// thread (src/rx_host_corr.cu:143-175).  This server keeps several array
+// streams of different sizes resident on one GPU:
+//   * admission (mixer_server_open) reserves a stream's device state -- its
+//     packet staging ring, corner-turn planes, int64 integration cube and
+//     FP32 dump cube -- against a device-memory budget and a slot count, and
+//     refuses with MIXER_EBUSY when either is exhausted; closing a stream
+//     returns both, so a later open is admitted;
+//   * mixer_server_submit copies heaps (host or device packets) into the
+//     stream's ring on a copy stream;
+//   * one worker thread runs the continuous-batching loop: every iteration it
+//     takes the complete sub-integrations of ALL streams that have any, runs
+//     their corner-turns, and then a single persistent k_xcorr_tri launch whose
+//     work list holds every ready stream's (channel, tile) items, so streams
+//     that arrive while others are on the GPU join the next launch;
+//   * after nsub_dump sub-integrations a stream's int64 cube is unpacked into
+//     its FP32 dump cube, copied to pinned host memory on a separate stream,
+//     and zeroed; a host callback stamps the completion time, giving the dump
+//     latency from the submission of the dump's last heap.
+// Every stream's arithmetic is exactly that of mixer_correlate on the same
+// packets, so a stream's dumps are identical alone and in any mix.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+#include "xcorr.cuh"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double now_s() {
+    return std::chrono::duration<double>(Clock::now().time_since_epoch()).count();
+}
+
+constexpr int kDumpSlots = 2;
+
+struct DumpSlot {
+    float* host = nullptr;          // pinned FP32 cube
+    int state = 0;                  // 0 free, 1 in flight, 2 ready
+    int64_t index = 0;
+    double t_last_submit = 0.0;
+    std::atomic<double> t_done{0.0};
+};
+
+struct Stream {
+    bool used = false;
+    bool closing = false;
+    mixer_array_desc d;
+    int64_t bytes = 0;
+    int64_t hps = 0;                // heaps per sub-integration
+    int64_t ring_subs = 0;
+    int64_t batch_subs = 0;         // most sub-integrations per launch
+    int64_t heap_bytes = 0;
+    uint8_t* ring = nullptr;
+    int8_t* planes = nullptr;
+    int64_t kt = 0;
+    int64_t* vis = nullptr;
+    float* dump_dev = nullptr;
+    uint32_t* d_seq_err = nullptr;
+    CUtensorMap map;
+    std::vector<cudaEvent_t> ev_ready;   // per ring slot: its heaps are on the device
+    std::vector<cudaEvent_t> ev_free;    // per ring slot: its corner-turn is done
+    std::vector<double> t_slot_done;     // per ring slot: host time its last heap arrived
+    std::vector<bool> slot_free_valid;
+    cudaEvent_t ev_dump_copied = nullptr;
+    cudaEvent_t ev_dump_kernel = nullptr;
+    bool dump_copy_pending = false;
+    DumpSlot dump[kDumpSlots];
+    int64_t heaps_in = 0;           // heaps submitted
+    int64_t subs_done = 0;          // sub-integrations taken by the worker
+    int64_t subs_in_dump = 0;
+    int64_t dumps_emitted = 0;
+    int64_t dumps_dropped = 0;
+    int64_t bytes_in = 0;
+    uint32_t seq_next = 0;
+    bool seq_set = false;
+};
+
+}  // namespace
+
+struct mixer_server {
+    mixer_server_cfg cfg;
+    int dev = 0;
+    std::mutex mu;          // stream table, counters
+    std::mutex serve_mu;    // held by the worker for a whole iteration
+    std::condition_variable cv;
+    std::unique_ptr<Stream[]> streams;
+    int nstreams = 0;
+    int64_t bytes_used = 0;
+    int64_t admitted = 0, refused = 0, launches = 0, items = 0;
+    std::vector<double> latencies;
+    double t_first = 0.0, t_last = 0.0;
+    int64_t bytes_processed = 0;
+    cudaStream_t copy = nullptr, comp = nullptr, d2h = nullptr;
+    // double-buffered launch tables
+    CUtensorMap* d_maps[2] = {nullptr, nullptr};
+    mixer::XcorrProblem* d_probs[2] = {nullptr, nullptr};
+    mixer::XcorrWork* d_work[2] = {nullptr, nullptr};
+    int64_t work_cap[2] = {0, 0};
+    // pinned host copies of the tables, so the uploads are truly asynchronous
+    CUtensorMap* h_maps[2] = {nullptr, nullptr};
+    mixer::XcorrProblem* h_probs[2] = {nullptr, nullptr};
+    mixer::XcorrWork* h_work[2] = {nullptr, nullptr};
+    int64_t h_work_cap[2] = {0, 0};
+    cudaEvent_t table_free[2] = {nullptr, nullptr};
+    bool table_used[2] = {false, false};
+    int tsel = 0;
+    int32_t* d_err = nullptr;
+    std::thread worker;
+    std::atomic<bool> stop{false};
+    std::atomic<int> error{0};
+};
+
+namespace {
+
+struct DoneCtx {
+    DumpSlot* slot;
+};
+
+void CUDART_CB mark_done(void* p) {
+    DoneCtx* c = static_cast<DoneCtx*>(p);
+    c->slot->t_done.store(now_s());
+    delete c;
+}
+
+int64_t stream_bytes(const mixer_array_desc& d, int64_t ring_subs, int64_t batch_subs) {
+    const int64_t hps = d.ksub / d.tpkt;
+    const int64_t ring = ring_subs * hps * d.nant * (int64_t)d.pkt_stride;
+    const int64_t planes = 2LL * d.nch * d.nant * batch_subs * d.ksub;
+    const int64_t vis = mixer_vis_elems(d.nant, d.nch) * 8;
+    const int64_t dump = (int64_t)d.nch * 2 * d.nant * d.nant * 4;
+    return ring + planes + vis + dump + 4096;
+}
+
+void free_stream(Stream& s) {
+    cudaFree(s.ring);
+    cudaFree(s.planes);
+    cudaFree(s.vis);
+    cudaFree(s.dump_dev);
+    cudaFree(s.d_seq_err);
+    for (auto e : s.ev_ready) cudaEventDestroy(e);
+    for (auto e : s.ev_free) cudaEventDestroy(e);
+    if (s.ev_dump_copied) cudaEventDestroy(s.ev_dump_copied);
+    if (s.ev_dump_kernel) cudaEventDestroy(s.ev_dump_kernel);
+    for (auto& d : s.dump) cudaFreeHost(d.host);
+    s.ring = nullptr;
+    s.planes = nullptr;
+    s.vis = nullptr;
+    s.dump_dev = nullptr;
+    s.d_seq_err = nullptr;
+    s.ev_ready.clear();
+    s.ev_free.clear();
+    s.ev_dump_copied = nullptr;
+    s.ev_dump_kernel = nullptr;
+    for (auto& d : s.dump) {
+        d.host = nullptr;
+        d.state = 0;
+    }
+    s.used = false;
+    s.closing = false;
+}
+
+// One iteration of the continuous-batching loop.  Returns true if it did work.
+bool serve_once(mixer_server* sv) {
+    struct Ready {
+        int sid;
+        int64_t sub0, nsub;
+    };
+    std::vector<Ready> ready;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        for (int sid = 0; sid < sv->nstreams; ++sid) {
+            Stream& s = sv->streams[sid];
+            if (!s.used || s.closing) continue;
+            const int64_t full = s.heaps_in / s.hps;
+            int64_t n = full - s.subs_done;
+            if (n <= 0) continue;
+            n = std::min<int64_t>(n, s.batch_subs);
+            n = std::min<int64_t>(n, s.d.nsub_dump - s.subs_in_dump);   // stop at the dump edge
+            // a dump slot must be free before the edge is crossed
+            if (s.subs_in_dump + n == s.d.nsub_dump) {
+                bool free_slot = false;
+                for (auto& d : s.dump) free_slot |= (d.state == 0);
+                if (!free_slot) continue;
+            }
+            ready.push_back({sid, s.subs_done, n});
+        }
+    }
+    if (ready.empty()) return false;
+    cudaStream_t comp = sv->comp;
+    std::vector<CUtensorMap> maps;
+    std::vector<mixer::XcorrProblem> probs;
+    std::vector<mixer::XcorrWork> work;
+    for (size_t r = 0; r < ready.size(); ++r) {
+        Stream& s = sv->streams[ready[r].sid];
+        // corner-turn the ready sub-integrations, one launch per contiguous run of ring slots
+        for (int64_t q = 0; q < ready[r].nsub;) {
+            const int64_t sub = ready[r].sub0 + q;
+            const int64_t slot = sub % s.ring_subs;
+            const int64_t run = std::min<int64_t>(ready[r].nsub - q, s.ring_subs - slot);
+            cudaStreamWaitEvent(comp, s.ev_ready[slot + run - 1], 0);   // copies complete in order
+            const uint8_t* src = s.ring + slot * s.hps * s.heap_bytes;
+            const uint32_t seq = s.seq_next + (uint32_t)(sub * s.hps * s.d.nant);
+            mixer_corner_turn(src, s.d.pkt_stride, s.d.hdr_bytes, s.d.nant, s.d.nch, s.d.tpkt,
+                              (int32_t)(run * s.hps), seq, s.planes, s.kt, q * s.d.ksub, s.d_seq_err,
+                              sv->d_err, comp);
+            for (int64_t u = 0; u < run; ++u) cudaEventRecord(s.ev_free[slot + u], comp);
+            q += run;
+        }
+        const int nb = (s.d.nant + 127) / 128;
+        const int ntiles = nb * (nb + 1) / 2;
+        const int64_t klen = ready[r].nsub * s.d.ksub;
+        const uint32_t nkc = (uint32_t)((klen + 127) / 128);
+        CUtensorMap m;
+        mixer::xcorr_encode_map(&m, s.planes, s.d.nant, s.d.nch, s.kt, klen);
+        maps.push_back(m);
+        probs.push_back(mixer::XcorrProblem{s.d.nant, s.d.nch, ntiles, 0, MIXER_VIS_ACC_I64, 0, s.vis});
+        for (int32_t c = 0; c < s.d.nch; ++c)
+            for (int t = 0; t < ntiles; ++t) {
+                mixer::XcorrWork it;
+                it.prob = (uint16_t)r;
+                it.tile = (uint16_t)t;
+                it.chan = (uint32_t)c;
+                it.kc0 = 0;
+                it.nkc = nkc;
+                work.push_back(it);
+            }
+    }
+    std::stable_sort(work.begin(), work.end(),
+                     [](const mixer::XcorrWork& a, const mixer::XcorrWork& b) { return a.nkc > b.nkc; });
+    // tables: reuse set tsel once its previous launch finished
+    const int ts = sv->tsel;
+    sv->tsel ^= 1;
+    if (sv->table_used[ts]) cudaEventSynchronize(sv->table_free[ts]);
+    const size_t np = probs.size();
+    if ((int64_t)work.size() > sv->work_cap[ts]) {
+        cudaFree(sv->d_work[ts]);
+        cudaFreeHost(sv->h_work[ts]);
+        const size_t cap = work.size() + work.size() / 2;
+        cudaMalloc(&sv->d_work[ts], cap * sizeof(mixer::XcorrWork));
+        cudaMallocHost(&sv->h_work[ts], cap * sizeof(mixer::XcorrWork));
+        sv->work_cap[ts] = (int64_t)cap;
+    }
+    memcpy(sv->h_maps[ts], maps.data(), np * sizeof(CUtensorMap));
+    memcpy(sv->h_probs[ts], probs.data(), np * sizeof(mixer::XcorrProblem));
+    memcpy(sv->h_work[ts], work.data(), work.size() * sizeof(mixer::XcorrWork));
+    cudaMemcpyAsync(sv->d_maps[ts], sv->h_maps[ts], np * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
+                    comp);
+    cudaMemcpyAsync(sv->d_probs[ts], sv->h_probs[ts], np * sizeof(mixer::XcorrProblem),
+                    cudaMemcpyHostToDevice, comp);
+    cudaMemcpyAsync(sv->d_work[ts], sv->h_work[ts], work.size() * sizeof(mixer::XcorrWork),
+                    cudaMemcpyHostToDevice, comp);
+    const int rc = mixer::xcorr_launch_table(sv->d_maps[ts], sv->d_probs[ts], sv->d_work[ts],
+                                             (int64_t)work.size(), mixer::xcorr_sm_count(), sv->d_err,
+                                             comp);
+    if (rc != MIXER_OK) sv->error.store(rc);
+    cudaEventRecord(sv->table_free[ts], comp);
+    sv->table_used[ts] = true;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->launches += 1;
+    sv->items += (int64_t)work.size();
+    for (const Ready& r : ready) {
+        Stream& s = sv->streams[r.sid];
+        s.subs_done += r.nsub;
+        s.subs_in_dump += r.nsub;
+        sv->bytes_processed += r.nsub * s.hps * s.heap_bytes;
+        if (s.subs_in_dump < s.d.nsub_dump) continue;
+        // dump edge: FP32 cube, D2H, zero the cube
+        int slot = -1;
+        for (int q = 0; q < kDumpSlots; ++q)
+            if (s.dump[q].state == 0) {
+                slot = q;
+                break;
+            }
+        DumpSlot& ds = s.dump[slot];
+        if (s.dump_copy_pending) cudaStreamWaitEvent(comp, s.ev_dump_copied, 0);
+        mixer_vis_dump_f32(s.vis, s.d.nant, s.d.nch, s.dump_dev, comp);
+        cudaMemsetAsync(s.vis, 0, (size_t)mixer_vis_elems(s.d.nant, s.d.nch) * 8, comp);
+        cudaEventRecord(s.ev_dump_kernel, comp);
+        cudaStreamWaitEvent(sv->d2h, s.ev_dump_kernel, 0);
+        const size_t nbytes = (size_t)s.d.nch * 2 * s.d.nant * s.d.nant * sizeof(float);
+        cudaMemcpyAsync(ds.host, s.dump_dev, nbytes, cudaMemcpyDeviceToHost, sv->d2h);
+        cudaEventRecord(s.ev_dump_copied, sv->d2h);
+        s.dump_copy_pending = true;
+        ds.state = 1;
+        ds.index = s.dumps_emitted++;
+        ds.t_last_submit = s.t_slot_done[(s.subs_done - 1) % s.ring_subs];
+        ds.t_done.store(0.0);
+        cudaLaunchHostFunc(sv->d2h, mark_done, new DoneCtx{&ds});
+        s.subs_in_dump = 0;
+    }
+    return true;
+}
+
+void collect_done(mixer_server* sv) {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    for (int q = 0; q < sv->nstreams; ++q) {
+        Stream& s = sv->streams[q];
+        if (!s.used) continue;
+        for (auto& d : s.dump) {
+            if (d.state == 1) {
+                const double t = d.t_done.load();
+                if (t > 0.0) {
+                    d.state = 2;
+                    sv->latencies.push_back(t - d.t_last_submit);
+                    sv->t_last = std::max(sv->t_last, t);
+                }
+            }
+        }
+    }
+}
+
+void worker_main(mixer_server* sv) {
+    cudaSetDevice(sv->dev);
+    while (!sv->stop.load()) {
+        bool did;
+        {
+            std::lock_guard<std::mutex> it(sv->serve_mu);
+            did = serve_once(sv);
+        }
+        collect_done(sv);
+        if (!did) {
+            std::unique_lock<std::mutex> lk(sv->mu);
+            sv->cv.wait_for(lk, std::chrono::microseconds(200));
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" int64_t mixer_server_stream_bytes(const mixer_server_cfg* cfg, const mixer_array_desc* d) {
+    if (!cfg || !d || d->tpkt <= 0 || d->ksub <= 0) return -1;
+    const int64_t batch_subs = std::max<int64_t>(
+        1, std::min<int64_t>(cfg->batch_subs > 0 ? cfg->batch_subs : 4, MIXER_KMAX_I32 / d->ksub));
+    const int64_t ring_subs = std::max<int64_t>(cfg->ring_subs > 0 ? cfg->ring_subs : 8, 2);
+    return stream_bytes(*d, ring_subs, batch_subs);
+}
+
+extern "C" int mixer_server_create(const mixer_server_cfg* cfg, mixer_server** out) {
+    if (!cfg || !out || cfg->budget_bytes <= 0 || cfg->max_streams <= 0 || cfg->max_streams > 4096)
+        return MIXER_EINVAL;
+    *out = nullptr;
+    mixer_server* sv = new mixer_server();
+    sv->cfg = *cfg;
+    if (sv->cfg.ring_subs <= 0) sv->cfg.ring_subs = 8;
+    if (sv->cfg.batch_subs <= 0) sv->cfg.batch_subs = 4;
+    sv->streams.reset(new Stream[cfg->max_streams]);
+    sv->nstreams = cfg->max_streams;
+    cudaError_t e;
+    auto fail = [&](cudaError_t err, const char* what) {
+        const int r = mixer::cuda_status(err, what);
+        mixer_server_destroy(sv);
+        return r;
+    };
+    if ((e = cudaGetDevice(&sv->dev)) != cudaSuccess) return fail(e, "cudaGetDevice");
+    if ((e = cudaStreamCreateWithFlags(&sv->copy, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&sv->comp, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&sv->d2h, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(e, "server streams");
+    for (int t = 0; t < 2; ++t) {
+        if ((e = cudaMalloc(&sv->d_maps[t], cfg->max_streams * sizeof(CUtensorMap))) != cudaSuccess ||
+            (e = cudaMalloc(&sv->d_probs[t], cfg->max_streams * sizeof(mixer::XcorrProblem))) != cudaSuccess ||
+            (e = cudaMallocHost(&sv->h_maps[t], cfg->max_streams * sizeof(CUtensorMap))) != cudaSuccess ||
+            (e = cudaMallocHost(&sv->h_probs[t], cfg->max_streams * sizeof(mixer::XcorrProblem))) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&sv->table_free[t], cudaEventDisableTiming)) != cudaSuccess)
+            return fail(e, "server tables");
+    }
+    if ((e = cudaMalloc(&sv->d_err, sizeof(int32_t))) != cudaSuccess ||
+        (e = cudaMemset(sv->d_err, 0, sizeof(int32_t))) != cudaSuccess)
+        return fail(e, "server error word");
+    sv->worker = std::thread(worker_main, sv);
+    *out = sv;
+    return MIXER_OK;
+}
+
+extern "C" int mixer_server_destroy(mixer_server* sv) {
+    if (!sv) return MIXER_OK;
+    sv->stop.store(true);
+    sv->cv.notify_all();
+    if (sv->worker.joinable()) sv->worker.join();
+    if (sv->comp) cudaStreamSynchronize(sv->comp);
+    if (sv->d2h) cudaStreamSynchronize(sv->d2h);
+    if (sv->copy) cudaStreamSynchronize(sv->copy);
+    for (int q = 0; q < sv->nstreams; ++q)
+        if (sv->streams[q].used) free_stream(sv->streams[q]);
+    for (int t = 0; t < 2; ++t) {
+        cudaFree(sv->d_maps[t]);
+        cudaFree(sv->d_probs[t]);
+        cudaFree(sv->d_work[t]);
+        cudaFreeHost(sv->h_maps[t]);
+        cudaFreeHost(sv->h_probs[t]);
+        cudaFreeHost(sv->h_work[t]);
+        if (sv->table_free[t]) cudaEventDestroy(sv->table_free[t]);
+    }
+    cudaFree(sv->d_err);
+    if (sv->copy) cudaStreamDestroy(sv->copy);
+    if (sv->comp) cudaStreamDestroy(sv->comp);
+    if (sv->d2h) cudaStreamDestroy(sv->d2h);
+    delete sv;
+    return MIXER_OK;
+}
+
+extern "C" int mixer_server_open(mixer_server* sv, const mixer_array_desc* d, int32_t* id) {
+    if (!sv || !d || !id) return MIXER_EINVAL;
+    if (d->nant <= 0 || d->nch <= 0 || d->tpkt <= 0 || d->tpkt % 16 || d->ksub <= 0 ||
+        d->ksub % d->tpkt || d->ksub % 128 || d->nsub_dump <= 0 || d->pkt_stride % 16 ||
+        d->hdr_bytes % 16 || d->hdr_bytes < 64 ||
+        (int64_t)d->hdr_bytes + 2LL * d->nch * d->tpkt > d->pkt_stride)
+        return MIXER_EINVAL;
+    const int64_t batch_subs = std::max<int64_t>(
+        1, std::min<int64_t>(sv->cfg.batch_subs, MIXER_KMAX_I32 / d->ksub));
+    const int64_t ring_subs = std::max<int64_t>(sv->cfg.ring_subs, 2);
+    const int64_t need = stream_bytes(*d, ring_subs, batch_subs);
+    int sid = -1;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        for (int q = 0; q < sv->nstreams; ++q)
+            if (!sv->streams[q].used) {
+                sid = q;
+                break;
+            }
+        if (sid < 0 || sv->bytes_used + need > sv->cfg.budget_bytes) {
+            sv->refused += 1;
+            return MIXER_EBUSY;
+        }
+        sv->bytes_used += need;      // reserve before allocating
+        sv->streams[sid].used = true;
+        sv->streams[sid].closing = true;   // invisible to the worker until set up
+    }
+    Stream& s = sv->streams[sid];
+    s.d = *d;
+    s.bytes = need;
+    s.hps = d->ksub / d->tpkt;
+    s.ring_subs = ring_subs;
+    s.batch_subs = batch_subs;
+    s.heap_bytes = (int64_t)d->nant * d->pkt_stride;
+    s.kt = batch_subs * d->ksub;
+    s.heaps_in = s.subs_done = s.subs_in_dump = s.dumps_emitted = s.dumps_dropped = s.bytes_in = 0;
+    s.seq_set = false;
+    s.dump_copy_pending = false;
+    cudaError_t e = cudaSuccess;
+    const size_t dump_bytes = (size_t)d->nch * 2 * d->nant * d->nant * sizeof(float);
+    if ((e = cudaMalloc(&s.ring, ring_subs * s.hps * s.heap_bytes)) == cudaSuccess &&
+        (e = cudaMalloc(&s.planes, 2 * (size_t)d->nch * d->nant * s.kt)) == cudaSuccess &&
+        (e = cudaMalloc(&s.vis, (size_t)mixer_vis_elems(d->nant, d->nch) * 8)) == cudaSuccess &&
+        (e = cudaMemset(s.vis, 0, (size_t)mixer_vis_elems(d->nant, d->nch) * 8)) == cudaSuccess &&
+        (e = cudaMalloc(&s.dump_dev, dump_bytes)) == cudaSuccess &&
+        (e = cudaMalloc(&s.d_seq_err, sizeof(uint32_t))) == cudaSuccess &&
+        (e = cudaMemset(s.d_seq_err, 0, sizeof(uint32_t))) == cudaSuccess &&
+        (e = cudaEventCreateWithFlags(&s.ev_dump_copied, cudaEventDisableTiming)) == cudaSuccess &&
+        (e = cudaEventCreateWithFlags(&s.ev_dump_kernel, cudaEventDisableTiming)) == cudaSuccess) {
+        for (int q = 0; q < kDumpSlots && e == cudaSuccess; ++q) e = cudaMallocHost(&s.dump[q].host, dump_bytes);
+        s.ev_ready.assign(ring_subs, nullptr);
+        s.ev_free.assign(ring_subs, nullptr);
+        s.t_slot_done.assign(ring_subs, 0.0);
+        s.slot_free_valid.assign(ring_subs, false);
+        for (int64_t q = 0; q < ring_subs && e == cudaSuccess; ++q) {
+            e = cudaEventCreateWithFlags(&s.ev_ready[q], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.ev_free[q], cudaEventDisableTiming);
+        }
+    }
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (e != cudaSuccess) {
+        free_stream(s);
+        sv->bytes_used -= need;
+        return mixer::cuda_status(e, "mixer_server_open");
+    }
+    s.closing = false;
+    sv->admitted += 1;
+    *id = sid;
+    return MIXER_OK;
+}
+
+extern "C" int mixer_server_submit(mixer_server* sv, int32_t id, const void* packets, int64_t nheaps,
+                                   uint32_t seq0, int32_t on_device) {
+    if (!sv || !packets || nheaps <= 0 || id < 0 || id >= (int32_t)sv->nstreams) return MIXER_EINVAL;
+    if (sv->error.load()) return sv->error.load();
+    int64_t h0, ring_heaps, hps;
+    Stream* sp;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        Stream& s = sv->streams[id];
+        if (!s.used || s.closing) return MIXER_EINVAL;
+        ring_heaps = s.ring_subs * s.hps;
+        hps = s.hps;
+        // heaps the worker has not taken yet occupy the ring
+        if (s.heaps_in + nheaps - s.subs_done * s.hps > ring_heaps) return MIXER_EBUSY;
+        if (!s.seq_set) {
+            s.seq_next = seq0;
+            s.seq_set = true;
+        }
+        h0 = s.heaps_in;
+        sp = &s;
+    }
+    Stream& s = *sp;
+    if (sv->t_first == 0.0) sv->t_first = now_s();
+    const uint8_t* src = static_cast<const uint8_t*>(packets);
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    int64_t done = 0;
+    while (done < nheaps) {
+        const int64_t h = h0 + done;
+        const int64_t pos = h % ring_heaps;
+        const int64_t slot = pos / hps;
+        // the slot may still be read by an earlier corner-turn
+        if (pos % hps == 0 && s.slot_free_valid[slot]) cudaStreamWaitEvent(sv->copy, s.ev_free[slot], 0);
+        const int64_t n = std::min<int64_t>(nheaps - done, hps - pos % hps);
+        MIXER_CK(cudaMemcpyAsync(s.ring + pos * s.heap_bytes, src + done * s.heap_bytes,
+                                 (size_t)(n * s.heap_bytes), kind, sv->copy));
+        done += n;
+        if ((h0 + done) % hps == 0) {   // slot complete
+            MIXER_CK(cudaEventRecord(s.ev_ready[slot], sv->copy));
+            s.slot_free_valid[slot] = true;
+            s.t_slot_done[slot] = now_s();
+        }
+    }
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        s.heaps_in += nheaps;
+        s.bytes_in += nheaps * s.heap_bytes;
+    }
+    sv->cv.notify_one();
+    return MIXER_OK;
+}
+
+extern "C" int mixer_server_poll(mixer_server* sv, int32_t id, mixer_dump_info* info, float* out) {
+    if (!sv || !info || id < 0 || id >= (int32_t)sv->nstreams) return MIXER_EINVAL;
+    collect_done(sv);
+    std::lock_guard<std::mutex> lk(sv->mu);
+    Stream& s = sv->streams[id];
+    memset(info, 0, sizeof(*info));
+    if (!s.used) return MIXER_EINVAL;
+    DumpSlot* best = nullptr;
+    for (auto& d : s.dump)
+        if (d.state == 2 && (!best || d.index < best->index)) best = &d;
+    if (!best) return MIXER_OK;
+    info->available = 1;
+    info->index = best->index;
+    info->latency_s = best->t_done.load() - best->t_last_submit;
+    info->nch = s.d.nch;
+    info->nant = s.d.nant;
+    if (out) memcpy(out, best->host, (size_t)s.d.nch * 2 * s.d.nant * s.d.nant * sizeof(float));
+    best->state = 0;
+    return MIXER_OK;
+}
+
+extern "C" int mixer_server_close(mixer_server* sv, int32_t id) {
+    if (!sv || id < 0 || id >= (int32_t)sv->nstreams) return MIXER_EINVAL;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        Stream& s = sv->streams[id];
+        if (!s.used || s.closing) return MIXER_EINVAL;
+        s.closing = true;   // the worker stops scheduling it
+    }
+    // the worker's current iteration may still enqueue work for this stream:
+    // wait for it to end (later iterations skip a closing stream), then drain
+    { std::lock_guard<std::mutex> it(sv->serve_mu); }
+    cudaStreamSynchronize(sv->copy);
+    cudaStreamSynchronize(sv->comp);
+    cudaStreamSynchronize(sv->d2h);
+    collect_done(sv);
+    std::lock_guard<std::mutex> lk(sv->mu);
+    Stream& s = sv->streams[id];
+    sv->bytes_used -= s.bytes;
+    free_stream(s);
+    return MIXER_OK;
+}
+
+extern "C" int mixer_server_stats(mixer_server* sv, mixer_server_counters* st) {
+    if (!sv || !st) return MIXER_EINVAL;
+    collect_done(sv);
+    std::lock_guard<std::mutex> lk(sv->mu);
+    memset(st, 0, sizeof(*st));
+    st->admitted = sv->admitted;
+    st->refused = sv->refused;
+    st->launches = sv->launches;
+    st->work_items = sv->items;
+    st->bytes_used = sv->bytes_used;
+    st->bytes_processed = sv->bytes_processed;
+    st->dumps = (int64_t)sv->latencies.size();
+    if (!sv->latencies.empty()) {
+        std::vector<double> l = sv->latencies;
+        std::sort(l.begin(), l.end());
+        auto pct = [&](double p) {
+            const size_t i = (size_t)std::min<double>((double)l.size() - 1, p * (double)(l.size() - 1) + 0.5);
+            return l[i];
+        };
+        st->p50_latency_s = pct(0.50);
+        st->p99_latency_s = pct(0.99);
+        st->max_latency_s = l.back();
+    }
+    st->elapsed_s = (sv->t_first > 0.0) ? now_s() - sv->t_first : 0.0;
+    int32_t ke = 0;
+    cudaMemcpy(&ke, sv->d_err, sizeof(ke), cudaMemcpyDeviceToHost);
+    st->kernel_err = ke;
+    int64_t se = 0;
+    for (int q = 0; q < sv->nstreams; ++q) {
+        Stream& s = sv->streams[q];
+        if (s.used && s.d_seq_err) {
+            uint32_t v = 0;
+            cudaMemcpy(&v, s.d_seq_err, sizeof(v), cudaMemcpyDeviceToHost);
+            se += v;
+        }
+    }
+    st->seq_errors = se;
+    return sv->error.load() ? sv->error.load() : (ke ? MIXER_ETIMEOUT : MIXER_OK);
+}

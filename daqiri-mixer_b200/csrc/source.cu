@@ -156,8 +156,30 @@ Hdr64 make_header(int wire_bytes, uint16_t port) {
     return h;
 }
 
+__global__ void k_restamp(uint8_t* __restrict__ pk, int64_t npk, int64_t stride, uint32_t seq0) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npk) return;
+    const uint32_t s = seq0 + (uint32_t)p;
+    uint8_t* h = pk + p * stride + MIXER_WIRE_SEQ_BYTE;
+    h[0] = (uint8_t)(s >> 24);
+    h[1] = (uint8_t)(s >> 16);
+    h[2] = (uint8_t)(s >> 8);
+    h[3] = (uint8_t)s;
+}
+
 }  // namespace
 }  // namespace mixer
+
+extern "C" int mixer_restamp_seq(uint8_t* packets, int64_t npk, int64_t pkt_stride, uint32_t seq0,
+                                 void* stream) {
+    if (!packets || npk <= 0 || pkt_stride < 64) return MIXER_EINVAL;
+    const int64_t blocks = (npk + 255) / 256;
+    if (blocks > 0x7FFFFFFFLL) return MIXER_EINVAL;
+    mixer::k_restamp<<<(unsigned)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(packets, npk,
+                                                                                      pkt_stride, seq0);
+    MIXER_CK(cudaGetLastError());
+    return MIXER_OK;
+}
 
 extern "C" int mixer_sky_table(int32_t nant, int32_t nch, int32_t side_x, int32_t nsrc,
                                const double* l, const double* m, const double* amp0,

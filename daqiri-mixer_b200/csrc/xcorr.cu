@@ -27,6 +27,8 @@
 //   warp 1      TMEM allocator + MMA issuer
 //   warps 2..5  epilogue (TMEM lane quadrant = warp % 4)
 #include "common.cuh"
+#include "xcorr.cuh"
+#include <cstring>
 
 namespace mixer {
 
@@ -47,9 +49,13 @@ struct XcorrArgs {
     int32_t kbeg, nkc;   // first sample, number of 128-sample chunks
     int32_t mode;
     int32_t pad_;
-    int64_t nwork;       // nch * ntiles
+    int64_t nwork;       // nch * ntiles, or the length of `work`
     void* vis;
     int32_t* err;
+    // Batched mode (work != nullptr): per-array tensor maps, problems, work list.
+    const CUtensorMap* tmaps;
+    const XcorrProblem* probs;
+    const XcorrWork* work;
 };
 
 __device__ __forceinline__ void decode_tile(int t, int& i, int& j) {
@@ -58,6 +64,41 @@ __device__ __forceinline__ void decode_tile(int t, int& i, int& j) {
     while (ii * (ii + 1) / 2 > t) --ii;
     i = ii;
     j = t - ii * (ii + 1) / 2;
+}
+
+struct Item {
+    const CUtensorMap* map;
+    void* vis;
+    int c, t, i, j, kbeg, kc0, nkc, mode, ntiles;
+};
+
+__device__ __forceinline__ Item get_item(const XcorrArgs& a, const CUtensorMap* pmap, int64_t w) {
+    Item it;
+    if (a.work == nullptr) {
+        it.c = (int)(w / a.ntiles);
+        it.t = (int)(w - (int64_t)it.c * a.ntiles);
+        it.map = pmap;
+        it.vis = a.vis;
+        it.kbeg = a.kbeg;
+        it.kc0 = 0;
+        it.nkc = a.nkc;
+        it.mode = a.mode;
+        it.ntiles = a.ntiles;
+    } else {
+        const XcorrWork wk = a.work[w];
+        const XcorrProblem& pr = a.probs[wk.prob];
+        it.c = (int)wk.chan;
+        it.t = (int)wk.tile;
+        it.map = a.tmaps + wk.prob;
+        it.vis = pr.vis;
+        it.kbeg = pr.kbeg;
+        it.kc0 = (int)wk.kc0;
+        it.nkc = (int)wk.nkc;
+        it.mode = pr.mode;
+        it.ntiles = pr.ntiles;
+    }
+    decode_tile(it.t, it.i, it.j);
+    return it;
 }
 
 // Four 32x32b.x16 TMEM loads and the wait, in one asm statement so no use of
@@ -118,7 +159,7 @@ __global__ void __launch_bounds__(192, 1)
         *abort_flag = 0;
         fence_mbar_init();
     }
-    if (warp == 0 && lane == 0) prefetch_tmap(&tmap);
+    if (warp == 0 && lane == 0 && args.work == nullptr) prefetch_tmap(&tmap);
     if (warp == 1) {
         tmem_alloc(smem_u32(tmem_slot), kTmemCols);
         tmem_relinquish();
@@ -136,13 +177,10 @@ __global__ void __launch_bounds__(192, 1)
             int64_t issued = 0;
             bool ok = true;
             for (int64_t w = blockIdx.x; w < args.nwork && ok; w += gridDim.x) {
-                const int c = (int)(w / args.ntiles);
-                const int t = (int)(w - (int64_t)c * args.ntiles);
-                int i, j;
-                decode_tile(t, i, j);
-                const bool diag = (i == j);
+                const Item it = get_item(args, &tmap, w);
+                const bool diag = (it.i == it.j);
                 const uint32_t bytes = diag ? 2 * kTileBytes : 4 * kTileBytes;
-                for (int kc = 0; kc < args.nkc; ++kc) {
+                for (int kc = 0; kc < it.nkc; ++kc) {
                     if (!mbar_wait(bar(EMPTY + stage), phase ^ 1u, abort_flag)) {
                         ok = false;
                         break;
@@ -150,12 +188,12 @@ __global__ void __launch_bounds__(192, 1)
                     const uint32_t sb = base + stage * kStageBytes;
                     const uint32_t fb = bar(FULL + stage);
                     mbar_expect_tx(fb, bytes);
-                    const int k = args.kbeg + kc * kKc;
-                    tma_load_4d(sb + 0 * kTileBytes, &tmap, fb, k, i * kTile, c, 0);
-                    tma_load_4d(sb + 1 * kTileBytes, &tmap, fb, k, i * kTile, c, 1);
+                    const int k = it.kbeg + (it.kc0 + kc) * kKc;
+                    tma_load_4d(sb + 0 * kTileBytes, it.map, fb, k, it.i * kTile, it.c, 0);
+                    tma_load_4d(sb + 1 * kTileBytes, it.map, fb, k, it.i * kTile, it.c, 1);
                     if (!diag) {
-                        tma_load_4d(sb + 2 * kTileBytes, &tmap, fb, k, j * kTile, c, 0);
-                        tma_load_4d(sb + 3 * kTileBytes, &tmap, fb, k, j * kTile, c, 1);
+                        tma_load_4d(sb + 2 * kTileBytes, it.map, fb, k, it.j * kTile, it.c, 0);
+                        tma_load_4d(sb + 3 * kTileBytes, it.map, fb, k, it.j * kTile, it.c, 1);
                     }
                     ++issued;
                     if (++stage == kStages) {
@@ -180,17 +218,14 @@ __global__ void __launch_bounds__(192, 1)
             bool ok = true;
             const uint32_t t_d1 = tmem, t_d2 = tmem + 256;
             for (int64_t w = blockIdx.x; w < args.nwork; w += gridDim.x) {
-                const int c = (int)(w / args.ntiles);
-                const int t = (int)(w - (int64_t)c * args.ntiles);
-                int i, j;
-                decode_tile(t, i, j);
-                const bool diag = (i == j);
+                const Item it = get_item(args, &tmap, w);
+                const bool diag = (it.i == it.j);
                 if (!mbar_wait(bar(ACCE), acc_phase ^ 1u, abort_flag)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                for (int kc = 0; kc < args.nkc; ++kc) {
+                for (int kc = 0; kc < it.nkc; ++kc) {
                     if (!mbar_wait(bar(FULL + stage), phase, abort_flag)) {
                         ok = false;
                         break;
@@ -233,15 +268,14 @@ __global__ void __launch_bounds__(192, 1)
         const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
         uint32_t acc_phase = 0;
         for (int64_t w = blockIdx.x; w < args.nwork; w += gridDim.x) {
-            const int c = (int)(w / args.ntiles);
-            const int t = (int)(w - (int64_t)c * args.ntiles);
+            const Item it = get_item(args, &tmap, w);
             if (!mbar_wait(bar(ACCF), acc_phase, abort_flag)) {
                 if (args.err) atomicOr(args.err, 4);
                 *abort_flag = 1;
                 break;
             }
             tc_fence_after();
-            const size_t tb = ((size_t)c * args.ntiles + t) * (size_t)(2 * kTile * kTile);
+            const size_t tb = ((size_t)it.c * it.ntiles + it.t) * (size_t)(2 * kTile * kTile);
 #pragma unroll 1
             for (int n0 = 0; n0 < kTile; n0 += 16) {
                 uint32_t r[4][16];   // R1, P2, P1, R2
@@ -251,8 +285,8 @@ __global__ void __launch_bounds__(192, 1)
                     mbar_arrive(bar(ACCE));
                 }
                 const size_t e0 = tb + (size_t)n0 * kTile + m;
-                if (args.mode == MIXER_VIS_ACC_I64) {
-                    unsigned long long* v = reinterpret_cast<unsigned long long*>(args.vis);
+                if (it.mode == MIXER_VIS_ACC_I64) {
+                    unsigned long long* v = reinterpret_cast<unsigned long long*>(it.vis);
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
                         const int32_t vr = (int32_t)(r[0][e] + r[3][e]);
@@ -261,8 +295,8 @@ __global__ void __launch_bounds__(192, 1)
                         atomicAdd(v + e0 + (size_t)e * kTile + kTile * kTile,
                                   (unsigned long long)(long long)vi);
                     }
-                } else if (args.mode == MIXER_VIS_ACC_I32) {
-                    int* v = reinterpret_cast<int*>(args.vis);
+                } else if (it.mode == MIXER_VIS_ACC_I32) {
+                    int* v = reinterpret_cast<int*>(it.vis);
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
                         atomicAdd(v + e0 + (size_t)e * kTile, (int)(r[0][e] + r[3][e]));
@@ -270,7 +304,7 @@ __global__ void __launch_bounds__(192, 1)
                                   (int)(r[2][e] - r[1][e]));
                     }
                 } else {
-                    int* v = reinterpret_cast<int*>(args.vis);
+                    int* v = reinterpret_cast<int*>(it.vis);
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
                         v[e0 + (size_t)e * kTile] = (int)(r[0][e] + r[3][e]);
@@ -318,23 +352,23 @@ int sm_count() {
 
 }  // namespace
 
-// Launch over samples [kbeg, kbeg + klen) with klen <= MIXER_KMAX_I32.
-static int xcorr_launch(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt, int64_t kbeg,
-                        int64_t klen, int32_t mode, void* vis, int32_t* err, cudaStream_t st) {
+int xcorr_encode_map(CUtensorMap* map, const int8_t* planes, int32_t nant, int32_t nch, int64_t kt,
+                     int64_t kend) {
     EncodeFn enc = get_encode();
     if (!enc) return MIXER_ECUDA;
-    CUtensorMap map;
-    // dim 0 ends at kbeg + klen so the last chunk reads zeros past the range.
-    const cuuint64_t dims[4] = {(cuuint64_t)(kbeg + klen), (cuuint64_t)nant, (cuuint64_t)nch, 2};
+    // dim 0 ends at kend so the last chunk of a range reads zeros past it.
+    const cuuint64_t dims[4] = {(cuuint64_t)kend, (cuuint64_t)nant, (cuuint64_t)nch, 2};
     const cuuint64_t strides[3] = {(cuuint64_t)kt, (cuuint64_t)kt * nant,
                                    (cuuint64_t)kt * nant * nch};
     const cuuint32_t box[4] = {kKc, kTile, 1, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<int8_t*>(planes), dims,
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<int8_t*>(planes), dims,
                      strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return MIXER_EINVAL;
+    return r == CUDA_SUCCESS ? MIXER_OK : MIXER_EINVAL;
+}
 
+static int set_smem_attr() {
     static uint64_t attr_set = 0;   // one bit per device ordinal
     int dev = 0;
     MIXER_CK(cudaGetDevice(&dev));
@@ -343,6 +377,19 @@ static int xcorr_launch(const int8_t* planes, int32_t nant, int32_t nch, int64_t
                                       kSmemBytes));
         attr_set |= 1ull << dev;
     }
+    return MIXER_OK;
+}
+
+int xcorr_sm_count() { return sm_count(); }
+
+// Launch over samples [kbeg, kbeg + klen) with klen <= MIXER_KMAX_I32.
+static int xcorr_launch(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt, int64_t kbeg,
+                        int64_t klen, int32_t mode, void* vis, int32_t* err, cudaStream_t st) {
+    CUtensorMap map;
+    int rc = xcorr_encode_map(&map, planes, nant, nch, kt, kbeg + klen);
+    if (rc != MIXER_OK) return rc;
+    rc = set_smem_attr();
+    if (rc != MIXER_OK) return rc;
     XcorrArgs a;
     a.nant = nant;
     a.nch = nch;
@@ -355,8 +402,31 @@ static int xcorr_launch(const int8_t* planes, int32_t nant, int32_t nch, int64_t
     a.nwork = (int64_t)nch * a.ntiles;
     a.vis = vis;
     a.err = err;
+    a.tmaps = nullptr;
+    a.probs = nullptr;
+    a.work = nullptr;
     const int64_t grid = a.nwork < sm_count() ? a.nwork : sm_count();
     k_xcorr_tri<<<(unsigned)grid, 192, kSmemBytes, st>>>(map, a);
+    MIXER_CK(cudaGetLastError());
+    return MIXER_OK;
+}
+
+int xcorr_launch_table(const CUtensorMap* d_tmaps, const XcorrProblem* d_probs,
+                       const XcorrWork* d_work, int64_t nwork, int grid, int32_t* err,
+                       cudaStream_t st) {
+    if (nwork <= 0 || grid <= 0) return MIXER_EINVAL;
+    int rc = set_smem_attr();
+    if (rc != MIXER_OK) return rc;
+    XcorrArgs a;
+    memset(&a, 0, sizeof(a));
+    a.nwork = nwork;
+    a.err = err;
+    a.tmaps = d_tmaps;
+    a.probs = d_probs;
+    a.work = d_work;
+    CUtensorMap unused;
+    memset(&unused, 0, sizeof(unused));
+    k_xcorr_tri<<<(unsigned)(grid < nwork ? grid : nwork), 192, kSmemBytes, st>>>(unused, a);
     MIXER_CK(cudaGetLastError());
     return MIXER_OK;
 }

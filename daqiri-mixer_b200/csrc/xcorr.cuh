@@ -1,0 +1,32 @@
+// xcorr.cuh -- internal interface of the triangle cGEMM kernel for the batch
+// planner (batch.cu): device table entries and launch helpers.
+#pragma once
+#include "common.cuh"
+
+namespace mixer {
+
+// One array of a batched launch (device table entry).
+struct XcorrProblem {
+    int32_t nant, nch, ntiles, kbeg;   // kbeg: first sample of the array's range
+    int32_t mode, pad_;
+    void* vis;
+};
+// One work item: array `prob`, channel `chan`, lower-triangle tile `tile`,
+// 128-sample chunks [kc0, kc0 + nkc) of the array's range.
+struct XcorrWork {
+    uint16_t prob, tile;
+    uint32_t chan;
+    uint32_t kc0, nkc;
+};
+static_assert(sizeof(XcorrWork) == 16, "work item is 16 bytes");
+
+// Tensor map over planes [2][nch][nant][kt] whose sample dimension ends at kend.
+int xcorr_encode_map(CUtensorMap* map, const int8_t* planes, int32_t nant, int32_t nch, int64_t kt,
+                     int64_t kend);
+// One persistent launch over a device work list (`grid` CTAs at most).
+int xcorr_launch_table(const CUtensorMap* d_tmaps, const XcorrProblem* d_probs,
+                       const XcorrWork* d_work, int64_t nwork, int grid, int32_t* err,
+                       cudaStream_t st);
+int xcorr_sm_count();
+
+}  // namespace mixer

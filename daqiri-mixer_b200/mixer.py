@@ -54,6 +54,32 @@ _vp, _i32, _i64, _u32, _u16, _u64, _f64 = (C.c_void_p, C.c_int32, C.c_int64, C.c
                                            C.c_uint16, C.c_uint64, C.c_double)
 
 
+class XcorrProblem(C.Structure):
+    _fields_ = [("planes", _vp), ("nant", _i32), ("nch", _i32), ("kt", _i64), ("kbeg", _i64),
+                ("klen", _i64), ("mode", _i32), ("vis", _vp)]
+
+
+ORDER_LPT, ORDER_CHANNEL = 0, 1
+
+
+class ServerCfg(C.Structure):
+    _fields_ = [("budget_bytes", _i64), ("max_streams", _i32), ("ring_subs", _i32),
+                ("batch_subs", _i32)]
+
+
+class DumpInfo(C.Structure):
+    _fields_ = [("available", _i32), ("nant", _i32), ("nch", _i32), ("pad_", _i32),
+                ("index", _i64), ("latency_s", C.c_double)]
+
+
+class ServerCounters(C.Structure):
+    _fields_ = [("admitted", _i64), ("refused", _i64), ("launches", _i64), ("work_items", _i64),
+                ("bytes_used", _i64), ("bytes_processed", _i64), ("dumps", _i64),
+                ("seq_errors", _i64), ("p50_latency_s", C.c_double), ("p99_latency_s", C.c_double),
+                ("max_latency_s", C.c_double), ("elapsed_s", C.c_double), ("kernel_err", _i32),
+                ("pad_", _i32)]
+
+
 class ArrayDesc(C.Structure):
     _fields_ = [("nant", _i32), ("nch", _i32), ("tpkt", _i32), ("ksub", _i32),
                 ("nsub_dump", _i32), ("side_x", _i32), ("grid", _i32), ("pkt_stride", _i32),
@@ -83,7 +109,25 @@ _sig("mixer_image_noalloc", C.c_int, _vp, _i32, _i32, _i32, _i32, _vp, _vp, _vp,
 _sig("mixer_sky_table", C.c_int, _i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp)
 _sig("mixer_gen_packets", C.c_int, _vp, _i64, _i32, _i32, _i32, _i32, _i32, _i64, _u32, _u16, _vp,
      _f64, _u64, _i32, _vp)
+_sig("mixer_batch_create", C.c_int, C.POINTER(XcorrProblem), _i32, C.POINTER(_vp))
+_sig("mixer_batch_plan", C.c_int, _vp, C.POINTER(_i32), _i32, _i32)
+_sig("mixer_batch_autotune", C.c_int, _vp, _i32, _vp, C.POINTER(C.c_float))
+_sig("mixer_batch_run", C.c_int, _vp, _vp)
+_sig("mixer_batch_capture_graph", C.c_int, _vp, _vp)
+_sig("mixer_batch_replay", C.c_int, _vp, _vp)
+_sig("mixer_batch_info", C.c_int, _vp, C.POINTER(_i64), C.POINTER(_i32), C.POINTER(_i32),
+     C.POINTER(_i32))
+_sig("mixer_batch_destroy", C.c_int, _vp)
+_sig("mixer_restamp_seq", C.c_int, _vp, _i64, _i64, _u32, _vp)
 _sig("mixer_desc_default", C.c_int, C.POINTER(ArrayDesc))
+_sig("mixer_server_create", C.c_int, C.POINTER(ServerCfg), C.POINTER(_vp))
+_sig("mixer_server_destroy", C.c_int, _vp)
+_sig("mixer_server_stream_bytes", _i64, C.POINTER(ServerCfg), C.POINTER(ArrayDesc))
+_sig("mixer_server_open", C.c_int, _vp, C.POINTER(ArrayDesc), C.POINTER(_i32))
+_sig("mixer_server_close", C.c_int, _vp, _i32)
+_sig("mixer_server_submit", C.c_int, _vp, _i32, _vp, _i64, _u32, _i32)
+_sig("mixer_server_poll", C.c_int, _vp, _i32, C.POINTER(DumpInfo), _vp)
+_sig("mixer_server_stats", C.c_int, _vp, C.POINTER(ServerCounters))
 _sig("mixer_create", C.c_int, C.POINTER(ArrayDesc), C.POINTER(_vp))
 _sig("mixer_destroy", C.c_int, _vp)
 _sig("mixer_reset", C.c_int, _vp, _vp)
@@ -109,6 +153,11 @@ EXPORTED = [
     "mixer_correlate", "mixer_correlate_i32", "mixer_integrate", "mixer_dump",
     "mixer_dump_to_file", "mixer_read_vis_i64", "mixer_image", "mixer_stats", "mixer_state_ptr",
     "mixer_shm_open", "mixer_shm_publish", "mixer_shm_close",
+    "mixer_batch_create", "mixer_batch_plan", "mixer_batch_autotune", "mixer_batch_run",
+    "mixer_batch_capture_graph", "mixer_batch_replay", "mixer_batch_info", "mixer_batch_destroy",
+    "mixer_server_create", "mixer_server_destroy", "mixer_server_stream_bytes", "mixer_server_open",
+    "mixer_server_close", "mixer_server_submit", "mixer_server_poll", "mixer_server_stats",
+    "mixer_restamp_seq",
 ]
 
 
@@ -220,6 +269,11 @@ def gen_packets(packets, pkt_stride, hdr_bytes, nant, nch, tpkt, nheaps, heap0, 
            "mixer_gen_packets")
 
 
+def restamp_seq(packets, npk, pkt_stride, seq0, stream=None):
+    _check(_lib.mixer_restamp_seq(_ptr(packets), npk, pkt_stride, seq0 & 0xFFFFFFFF, _stream(stream)),
+           "mixer_restamp_seq")
+
+
 # ---- array context ------------------------------------------------------------
 
 def default_desc() -> ArrayDesc:
@@ -298,6 +352,134 @@ class ArrayContext:
 
     def state_ptr(self) -> int:
         return _lib.mixer_state_ptr(self._h)
+
+
+class Batch:
+    """Uneven arrays in one persistent launch (plan, autotune, graph replay).
+
+    problems: list of dicts with keys planes, nant, nch, kt, kbeg, klen, mode, vis.
+    """
+
+    def __init__(self, problems):
+        arr = (XcorrProblem * len(problems))()
+        for q, p in zip(arr, problems):
+            q.planes, q.nant, q.nch = _ptr(p["planes"]), p["nant"], p["nch"]
+            q.kt, q.kbeg, q.klen = p["kt"], p.get("kbeg", 0), p.get("klen", p["kt"])
+            q.mode, q.vis = p.get("mode", VIS_ACC_I64), _ptr(p["vis"])
+        self._keep = problems
+        h = _vp()
+        _check(_lib.mixer_batch_create(arr, len(problems), C.byref(h)), "mixer_batch_create")
+        self._h = h.value
+
+    def plan(self, split_per_class=(), order=ORDER_LPT):
+        n = len(split_per_class)
+        arr = (_i32 * max(n, 1))(*split_per_class)
+        _check(_lib.mixer_batch_plan(self._h, arr, n, order), "mixer_batch_plan")
+
+    def autotune(self, reps=2, stream=None) -> float:
+        ms = C.c_float()
+        _check(_lib.mixer_batch_autotune(self._h, reps, _stream(stream), C.byref(ms)),
+               "mixer_batch_autotune")
+        return ms.value
+
+    def run(self, stream=None):
+        _check(_lib.mixer_batch_run(self._h, _stream(stream)), "mixer_batch_run")
+
+    def capture_graph(self, stream):
+        _check(_lib.mixer_batch_capture_graph(self._h, _stream(stream)), "mixer_batch_capture_graph")
+
+    def replay(self, stream=None):
+        _check(_lib.mixer_batch_replay(self._h, _stream(stream)), "mixer_batch_replay")
+
+    def info(self):
+        n, o, e = _i64(), _i32(), _i32()
+        sp = (_i32 * 65)()
+        rc = _lib.mixer_batch_info(self._h, C.byref(n), C.byref(o), sp, C.byref(e))
+        if rc not in (OK, ETIMEOUT):
+            _check(rc, "mixer_batch_info")
+        return {"nwork": n.value, "order": o.value, "split": list(sp), "kernel_err": e.value}
+
+    def close(self):
+        if self._h:
+            _lib.mixer_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_desc(**kw) -> ArrayDesc:
+    d = default_desc()
+    for k, v in kw.items():
+        setattr(d, k, v)
+    return d
+
+
+class Server:
+    """Streaming X-engine: admission by memory budget, continuous batching, dumps."""
+
+    def __init__(self, budget_bytes, max_streams=16, ring_subs=0, batch_subs=0):
+        self.cfg = ServerCfg(budget_bytes, max_streams, ring_subs, batch_subs)
+        h = _vp()
+        _check(_lib.mixer_server_create(C.byref(self.cfg), C.byref(h)), "mixer_server_create")
+        self._h = h.value
+
+    def stream_bytes(self, desc: ArrayDesc) -> int:
+        return _lib.mixer_server_stream_bytes(C.byref(self.cfg), C.byref(desc))
+
+    def open(self, desc: ArrayDesc) -> int:
+        sid = _i32()
+        _check(_lib.mixer_server_open(self._h, C.byref(desc), C.byref(sid)), "mixer_server_open")
+        return sid.value
+
+    def try_open(self, desc: ArrayDesc):
+        sid = _i32()
+        rc = _lib.mixer_server_open(self._h, C.byref(desc), C.byref(sid))
+        if rc == EBUSY:
+            return None
+        _check(rc, "mixer_server_open")
+        return sid.value
+
+    def close_stream(self, sid: int):
+        _check(_lib.mixer_server_close(self._h, sid), "mixer_server_close")
+
+    def submit(self, sid, packets, nheaps, seq0=0, on_device=True) -> bool:
+        """False when the stream's staging ring is full (retry later)."""
+        rc = _lib.mixer_server_submit(self._h, sid, _ptr(packets), nheaps, seq0 & 0xFFFFFFFF,
+                                      1 if on_device else 0)
+        if rc == EBUSY:
+            return False
+        _check(rc, "mixer_server_submit")
+        return True
+
+    def poll(self, sid, out=None):
+        info = DumpInfo()
+        _check(_lib.mixer_server_poll(self._h, sid, C.byref(info), _ptr(out)), "mixer_server_poll")
+        if not info.available:
+            return None
+        return {"index": info.index, "latency_s": info.latency_s, "nant": info.nant,
+                "nch": info.nch}
+
+    def stats(self):
+        st = ServerCounters()
+        rc = _lib.mixer_server_stats(self._h, C.byref(st))
+        if rc not in (OK, ETIMEOUT):
+            _check(rc, "mixer_server_stats")
+        return {f: getattr(st, f) for f, _ in ServerCounters._fields_ if f != "pad_"}
+
+    def close(self):
+        if self._h:
+            _lib.mixer_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Corr32Shm:

@@ -185,6 +185,54 @@ int mixer_gen_packets(uint8_t* packets, int64_t pkt_stride, int32_t hdr_bytes,
                       const double* sky, double sigma, uint64_t seed,
                       int32_t noise_mode, void* stream);
 
+/* ---- batched persistent launch over uneven arrays ------------------------ */
+
+/* One array of a batch: planes as for mixer_xcorr_tri, samples
+ * [kbeg, kbeg + klen), accumulated into its own tile-packed cube `vis`. */
+typedef struct mixer_xcorr_problem {
+    const int8_t* planes;   /* int8 [2][nch][nant][kt] */
+    int32_t nant, nch;
+    int64_t kt, kbeg, klen;
+    int32_t mode;           /* MIXER_VIS_*; STORE_I32 items are never K-split */
+    void* vis;
+} mixer_xcorr_problem;
+
+typedef struct mixer_batch mixer_batch;
+
+#define MIXER_ORDER_LPT     0   /* items longest first (longest-processing-time) */
+#define MIXER_ORDER_CHANNEL 1   /* array, channel, tile order (L2 locality)       */
+
+/* Many independent arrays of different N, C and K in ONE persistent launch of
+ * the triangle cGEMM (no counterpart in the reference, which launches one
+ * fixed-shape kernel per V-update, src/rx_host_corr.cu:167).  The plan is a
+ * device work list of (array, channel, tile, K-chunk range) items; results
+ * are bit-identical to one mixer_xcorr_tri per array for every plan.
+ * The problem descriptors (planes, vis pointers) are captured at creation. */
+int mixer_batch_create(const mixer_xcorr_problem* probs, int32_t nprob, mixer_batch** out);
+/* Explicit plan: K-split factor per size class (class = ceil(nant / 128),
+ * index 0..nclass-1) and item order. */
+int mixer_batch_plan(mixer_batch* b, const int32_t* split_per_class, int32_t nclass, int32_t order);
+/* Autotuner: times candidate plans (order x greedy per-class K-split) on the
+ * caller's own buffers with `reps` launches each and keeps the fastest.  The
+ * ACC-mode cubes accumulate every trial: zero them afterwards. */
+int mixer_batch_autotune(mixer_batch* b, int32_t reps, void* stream, float* best_ms);
+/* One launch of the current plan. */
+int mixer_batch_run(mixer_batch* b, void* stream);
+/* Capture one launch of the current plan into a CUDA graph (stream must not be
+ * the legacy default stream); replay it with mixer_batch_replay.  Re-planning
+ * drops the graph. */
+int mixer_batch_capture_graph(mixer_batch* b, void* stream);
+int mixer_batch_replay(mixer_batch* b, void* stream);
+/* Plan and error word: nwork items, order, split_per_class[65]; kernel_err
+ * synchronises and returns MIXER_ETIMEOUT if a bounded wait gave up. */
+int mixer_batch_info(mixer_batch* b, int64_t* nwork, int32_t* order, int32_t* split_per_class,
+                     int32_t* kernel_err);
+int mixer_batch_destroy(mixer_batch* b);
+
+/* Rewrites the big-endian seq at byte 48 of npk packets to seq0, seq0+1, ...
+ * so a generated packet pool can be replayed as a continuing stream. */
+int mixer_restamp_seq(uint8_t* packets, int64_t npk, int64_t pkt_stride, uint32_t seq0, void* stream);
+
 /* ---- layer 2: array context --------------------------------------------- */
 
 typedef struct mixer_array_desc {
@@ -241,6 +289,62 @@ int mixer_image(mixer_ctx* ctx, float* img, float* vmax, float* vmin, int32_t de
 int mixer_stats(mixer_ctx* ctx, int64_t* samples, int64_t* seq_errors, int32_t* kernel_err);
 /* Raw device pointer of the int64 state (tile-packed). */
 int64_t* mixer_state_ptr(mixer_ctx* ctx);
+
+/* ---- streaming server: concurrent array streams, continuous batching ---- */
+
+typedef struct mixer_server_cfg {
+    int64_t budget_bytes;   /* device memory all admitted streams may reserve  */
+    int32_t max_streams;    /* stream slots                                    */
+    int32_t ring_subs;      /* staging depth per stream, sub-integrations (0: 8) */
+    int32_t batch_subs;     /* most sub-integrations of a stream per launch (0: 4) */
+} mixer_server_cfg;
+
+typedef struct mixer_dump_info {
+    int32_t available;      /* 1 if a dump was returned                        */
+    int32_t nant, nch;
+    int32_t pad_;
+    int64_t index;          /* dump number of that stream, from 0              */
+    double latency_s;       /* submit of its last heap -> dump in host memory  */
+} mixer_dump_info;
+
+typedef struct mixer_server_counters {
+    int64_t admitted, refused, launches, work_items;
+    int64_t bytes_used, bytes_processed, dumps, seq_errors;
+    double p50_latency_s, p99_latency_s, max_latency_s, elapsed_s;
+    int32_t kernel_err;
+    int32_t pad_;
+} mixer_server_counters;
+
+typedef struct mixer_server mixer_server;
+
+/* A serving loop with no counterpart in the reference (which serves one array
+ * from one NIC queue, src/rx_host_corr.cu:143-175).  Streams of different
+ * sizes are admitted against a device-memory budget and a slot count; a
+ * worker thread batches the complete sub-integrations of every stream into
+ * one persistent tensor-core launch per iteration (continuous batching);
+ * every nsub_dump sub-integrations a stream's FP32 dump cube [C][2][N][N]
+ * lands in pinned host memory.  A stream's dumps equal those of
+ * mixer_correlate + mixer_dump on the same packets, alone or in any mix.
+ * Stream descriptors need ksub % 128 == 0.  Calls are made with the
+ * server's device current. */
+int mixer_server_create(const mixer_server_cfg* cfg, mixer_server** out);
+int mixer_server_destroy(mixer_server* sv);
+/* Device bytes one stream of `d` reserves under `cfg`. */
+int64_t mixer_server_stream_bytes(const mixer_server_cfg* cfg, const mixer_array_desc* d);
+/* Admission: MIXER_EBUSY when the budget or the slots are exhausted. */
+int mixer_server_open(mixer_server* sv, const mixer_array_desc* d, int32_t* stream_id);
+/* Synchronises the server's streams, frees the stream's memory and slot. */
+int mixer_server_close(mixer_server* sv, int32_t stream_id);
+/* Queue nheaps heaps (nheaps * nant packets, h-major) of the stream, host or
+ * device memory; seq0 of the stream's first submission sets its expected
+ * sequence.  MIXER_EBUSY when its staging ring is full (retry later). */
+int mixer_server_submit(mixer_server* sv, int32_t stream_id, const void* packets, int64_t nheaps,
+                        uint32_t seq0, int32_t on_device);
+/* Oldest completed dump of the stream, copied to `out` (host, may be NULL to
+ * discard) and released; info->available = 0 when none is ready. */
+int mixer_server_poll(mixer_server* sv, int32_t stream_id, mixer_dump_info* info, float* out);
+/* Counters and p50 / p99 dump latency over all dumps so far. */
+int mixer_server_stats(mixer_server* sv, mixer_server_counters* st);
 
 /* Corr32 shared-memory publisher (src/rx_host_corr.cu:97-105,236): header
  * {u32 magic 0x43523343, w, h, nch; u64 write_seq} then img[nch][G][G],
