@@ -358,3 +358,19 @@ extern "C" int mixer_stats(mixer_ctx* c, int64_t* samples, int64_t* seq_errors, 
 }
 
 extern "C" int64_t* mixer_state_ptr(mixer_ctx* c) { return c ? c->vis64 : nullptr; }
+
+extern "C" int mixer_ctx_shape(mixer_ctx* c, int32_t* nant, int32_t* nch) {
+    if (!c) return MIXER_EINVAL;
+    if (nant) *nant = c->d.nant;
+    if (nch) *nch = c->d.nch;
+    return MIXER_OK;
+}
+
+extern "C" int mixer_write_vis_i64(mixer_ctx* c, const int64_t* tile_packed, int64_t samples) {
+    if (!c || !tile_packed || samples < 0) return MIXER_EINVAL;
+    MIXER_CK(cudaDeviceSynchronize());
+    MIXER_CK(cudaMemcpy(c->vis64, tile_packed, (size_t)c->vis_elems * sizeof(int64_t),
+                        cudaMemcpyHostToDevice));
+    c->samples = samples;
+    return MIXER_OK;
+}

@@ -119,6 +119,12 @@ _sig("mixer_batch_info", C.c_int, _vp, C.POINTER(_i64), C.POINTER(_i32), C.POINT
      C.POINTER(_i32))
 _sig("mixer_batch_destroy", C.c_int, _vp)
 _sig("mixer_restamp_seq", C.c_int, _vp, _i64, _i64, _u32, _vp)
+_sig("mixer_ctx_shape", C.c_int, _vp, C.POINTER(_i32), C.POINTER(_i32))
+_sig("mixer_write_vis_i64", C.c_int, _vp, _vp, _i64)
+_sig("mixer_state_save", C.c_int, _vp, C.c_char_p)
+_sig("mixer_state_load", C.c_int, _vp, C.c_char_p)
+_sig("mixer_align_heaps", C.c_int, _vp, _i64, _i64, _i32, C.POINTER(_i64), C.POINTER(_i64),
+     C.POINTER(_i64), C.POINTER(_u32))
 _sig("mixer_desc_default", C.c_int, C.POINTER(ArrayDesc))
 _sig("mixer_server_create", C.c_int, C.POINTER(ServerCfg), C.POINTER(_vp))
 _sig("mixer_server_destroy", C.c_int, _vp)
@@ -157,7 +163,8 @@ EXPORTED = [
     "mixer_batch_capture_graph", "mixer_batch_replay", "mixer_batch_info", "mixer_batch_destroy",
     "mixer_server_create", "mixer_server_destroy", "mixer_server_stream_bytes", "mixer_server_open",
     "mixer_server_close", "mixer_server_submit", "mixer_server_poll", "mixer_server_stats",
-    "mixer_restamp_seq",
+    "mixer_restamp_seq", "mixer_ctx_shape", "mixer_write_vis_i64", "mixer_state_save",
+    "mixer_state_load", "mixer_align_heaps",
 ]
 
 
@@ -274,6 +281,14 @@ def restamp_seq(packets, npk, pkt_stride, seq0, stream=None):
            "mixer_restamp_seq")
 
 
+def align_heaps(packets, npk, pkt_stride, nant):
+    """Host burst alignment: dict(first, nheaps, next, seq0)."""
+    f, n, x, s = _i64(), _i64(), _i64(), _u32()
+    _check(_lib.mixer_align_heaps(_ptr(packets), npk, pkt_stride, nant, C.byref(f), C.byref(n),
+                                  C.byref(x), C.byref(s)), "mixer_align_heaps")
+    return {"first": f.value, "nheaps": n.value, "next": x.value, "seq0": s.value}
+
+
 # ---- array context ------------------------------------------------------------
 
 def default_desc() -> ArrayDesc:
@@ -349,6 +364,12 @@ class ArrayContext:
         if rc not in (OK, ETIMEOUT):
             _check(rc, "mixer_stats")
         return {"samples": s.value, "seq_errors": e.value, "kernel_err": k.value}
+
+    def save(self, path: str):
+        _check(_lib.mixer_state_save(self._h, path.encode()), "mixer_state_save")
+
+    def load(self, path: str):
+        _check(_lib.mixer_state_load(self._h, path.encode()), "mixer_state_load")
 
     def state_ptr(self) -> int:
         return _lib.mixer_state_ptr(self._h)

@@ -346,6 +346,27 @@ int mixer_server_poll(mixer_server* sv, int32_t stream_id, mixer_dump_info* info
 /* Counters and p50 / p99 dump latency over all dumps so far. */
 int mixer_server_stats(mixer_server* sv, mixer_server_counters* st);
 
+/* Shape of a context's array. */
+int mixer_ctx_shape(mixer_ctx* ctx, int32_t* nant, int32_t* nch);
+/* Replaces the integration state with a host copy of the tile-packed int64
+ * cube and sets the integrated-sample counter (synchronous). */
+int mixer_write_vis_i64(mixer_ctx* ctx, const int64_t* tile_packed, int64_t samples);
+/* Checkpoint / resume of the int64 integration state (the reference zeroes
+ * its cube once and cannot resume, src/rx_host_corr.cu:188): a 32-byte
+ * header {"MIXCKPT1", nant, nch, samples, count} and the raw tile-packed
+ * cube.  Load refuses a file of another shape.  Synchronous. */
+int mixer_state_save(mixer_ctx* ctx, const char* path);
+int mixer_state_load(mixer_ctx* ctx, const char* path);
+
+/* Heap alignment of a packet burst in host memory, as the reference's drain
+ * thread does (src/rx_host_corr.cu:127-141), but checking every packet:
+ * *first = index of the first packet whose big-endian seq is a multiple of
+ * nant (*seq0 its seq), *nheaps = complete heaps of consecutive seqs from
+ * there, *next = where to resume (the first packet of a gap, or the packet
+ * after the last whole heap). */
+int mixer_align_heaps(const uint8_t* packets, int64_t npk, int64_t pkt_stride, int32_t nant,
+                      int64_t* first, int64_t* nheaps, int64_t* next, uint32_t* seq0);
+
 /* Corr32 shared-memory publisher (src/rx_host_corr.cu:97-105,236): header
  * {u32 magic 0x43523343, w, h, nch; u64 write_seq} then img[nch][G][G],
  * vmax[nch], vmin[nch].  name like "/corr32". */
