@@ -260,11 +260,29 @@ def run_sweep(args):
     import torch
     import mixer
     dev = torch.device("cuda:0")
-    for (N, C) in [(1024, 64), (4096, 8), (256, 128)]:
+    # library reference: cuBLASLt int8 GEMM through torch._int_mm, 8192^3
+    a = torch.randint(-128, 128, (8192, 8192), dtype=torch.int8, device=dev)
+    bt = torch.randint(-128, 128, (8192, 8192), dtype=torch.int8, device=dev)
+    for _ in range(3):
+        torch._int_mm(a, bt.t())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        torch._int_mm(a, bt.t())
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 10
+    print(json.dumps({"library": "torch._int_mm (cuBLASLt int8) 8192^3", "ms": ms,
+                      "tops": 2.0 * 8192 ** 3 / ms / 1e9}), flush=True)
+    del a, bt
+    shapes = [(1024, 64), (4096, 8)] if args.sweep_quick else [(1024, 64), (4096, 8), (256, 128)]
+    ks = [1024, 8192, 32768] if args.sweep_quick else [1024, 2048, 4096, 8192, 16384, 32768]
+    for (N, C) in shapes:
         n = mixer.vis_elems(N, C)
         v64 = torch.zeros(n, dtype=torch.int64, device=dev)
         v32 = torch.zeros(n, dtype=torch.int32, device=dev)
-        for K in [1024, 2048, 4096, 8192, 16384, 32768]:
+        for K in ks:
             planes = torch.randint(-128, 128, (2 * C * N * K,), dtype=torch.int8, device=dev)
             for mode, vis in [(mixer.VIS_STORE_I32, v32), (mixer.VIS_ACC_I64, v64)]:
                 for _ in range(2):
@@ -751,6 +769,7 @@ def main():
                     help="plain: the 1024-element array (headline); batched: 48 uneven arrays")
     ap.add_argument("--small-arrays", action="store_true",
                     help="batched config with arrays too small to fill the GPU alone")
+    ap.add_argument("--sweep-quick", action="store_true", help="fewer sweep points")
     ap.add_argument("--sweep-xcorr", action="store_true",
                     help="time the GEMM kernel over K and epilogue mode (JSON lines)")
     ap.add_argument("--profile", action="store_true",

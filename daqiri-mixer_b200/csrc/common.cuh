@@ -152,6 +152,15 @@ __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
            | ((uint64_t)2 << 61);                // layout: 128-byte swizzle
 }
 
+// Same for the 64-byte swizzle: rows of 64 bytes, 8-row groups 512 bytes apart.
+__device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu)   // start address / 16
+           | ((uint64_t)1 << 16)                 // leading byte offset (unused here)
+           | ((uint64_t)(512 >> 4) << 32)        // stride byte offset: 8 rows
+           | ((uint64_t)1 << 46)                 // descriptor version (sm_100)
+           | ((uint64_t)4 << 61);                // layout: 64-byte swizzle
+}
+
 #endif  // __CUDACC__
 
 }  // namespace mixer

@@ -34,11 +34,31 @@ namespace mixer {
 
 namespace {
 
+// Pipeline geometry (build-time options): samples per stage (128 with the
+// 128-byte swizzle or 64 with the 64-byte swizzle), stage count, and epilogue
+// warps per TMEM lane quadrant.
+#ifndef MIXER_XCORR_KC
+#define MIXER_XCORR_KC 128
+#endif
+#ifndef MIXER_XCORR_STAGES
+#define MIXER_XCORR_STAGES 3
+#endif
+#ifndef MIXER_XCORR_EPI_GROUPS
+#define MIXER_XCORR_EPI_GROUPS 2
+#endif
 constexpr int kTile = 128;                       // tile rows = cols
-constexpr int kKc = 128;                         // samples (bytes) per stage
-constexpr int kStages = 3;
-constexpr int kTileBytes = kTile * kKc;          // 16 KiB
+constexpr int kWorkChunk = 128;                  // samples per work-list K unit
+constexpr int kKc = MIXER_XCORR_KC;              // samples (bytes) per pipeline stage
+constexpr int kSubPerChunk = kWorkChunk / kKc;
+constexpr int kStages = MIXER_XCORR_STAGES;
+constexpr int kTileBytes = kTile * kKc;
 constexpr int kStageBytes = 4 * kTileBytes;      // Ar, Ai, Br, Bi
+static_assert(kKc == 64 || kKc == 128, "stage of 64 or 128 samples");
+static_assert(kStages * kStageBytes + 1024 + 256 <= 232448, "shared memory");
+constexpr int kEpiGroups = MIXER_XCORR_EPI_GROUPS;  // column groups per TMEM lane quadrant
+constexpr int kEpiWarps = 4 * kEpiGroups;
+constexpr int kEpiCols = kTile / kEpiGroups;     // 64 columns per warp
+constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr int kBarBytes = 256;
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 + kBarBytes;
 constexpr uint32_t kTmemCols = 512;              // D1 (256) + D2 (256)
@@ -64,6 +84,10 @@ __device__ __forceinline__ void decode_tile(int t, int& i, int& j) {
     while (ii * (ii + 1) / 2 > t) --ii;
     i = ii;
     j = t - ii * (ii + 1) / 2;
+}
+
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+    return kKc == 128 ? sdesc_sw128(saddr) : sdesc_sw64(saddr);
 }
 
 struct Item {
@@ -101,8 +125,8 @@ __device__ __forceinline__ Item get_item(const XcorrArgs& a, const CUtensorMap* 
     return it;
 }
 
-// Four 32x32b.x16 TMEM loads and the wait, in one asm statement so no use of
-// the results can be scheduled before the wait.
+// Four 32x32b.x16 TMEM loads (16 columns each) and the wait, in one asm
+// statement so no use of the results can be scheduled before the wait.
 __device__ __forceinline__ void tmem_ld4_x16(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
                                              uint32_t (&r)[4][16]) {
     asm volatile(
@@ -132,11 +156,11 @@ __device__ __forceinline__ void tmem_ld4_x16(uint32_t a0, uint32_t a1, uint32_t 
         : "memory");
 }
 
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(kThreads, 1)
     k_xcorr_tri(const __grid_constant__ CUtensorMap tmap, const XcorrArgs args) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
-    const uint32_t base = (raw + 1023u) & ~1023u;           // 1 KiB aligned for SW128
+    const uint32_t base = (raw + 1023u) & ~1023u;           // 1 KiB aligned (swizzle atoms)
     uint8_t* gbase = smem_raw + (base - raw);
     uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + kStages * kStageBytes);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 4);
@@ -154,7 +178,7 @@ __global__ void __launch_bounds__(192, 1)
             mbar_init(bar(EMPTY + s), 1);
         }
         mbar_init(bar(ACCF), 1);
-        mbar_init(bar(ACCE), 128);
+        mbar_init(bar(ACCE), 32 * kEpiWarps);
         mbar_init(bar(DRAIN), 1);
         *abort_flag = 0;
         fence_mbar_init();
@@ -180,7 +204,7 @@ __global__ void __launch_bounds__(192, 1)
                 const Item it = get_item(args, &tmap, w);
                 const bool diag = (it.i == it.j);
                 const uint32_t bytes = diag ? 2 * kTileBytes : 4 * kTileBytes;
-                for (int kc = 0; kc < it.nkc; ++kc) {
+                for (int kc = 0; kc < it.nkc * kSubPerChunk; ++kc) {
                     if (!mbar_wait(bar(EMPTY + stage), phase ^ 1u, abort_flag)) {
                         ok = false;
                         break;
@@ -188,7 +212,7 @@ __global__ void __launch_bounds__(192, 1)
                     const uint32_t sb = base + stage * kStageBytes;
                     const uint32_t fb = bar(FULL + stage);
                     mbar_expect_tx(fb, bytes);
-                    const int k = it.kbeg + (it.kc0 + kc) * kKc;
+                    const int k = it.kbeg + it.kc0 * kWorkChunk + kc * kKc;
                     tma_load_4d(sb + 0 * kTileBytes, it.map, fb, k, it.i * kTile, it.c, 0);
                     tma_load_4d(sb + 1 * kTileBytes, it.map, fb, k, it.i * kTile, it.c, 1);
                     if (!diag) {
@@ -225,17 +249,17 @@ __global__ void __launch_bounds__(192, 1)
                     break;
                 }
                 tc_fence_after();
-                for (int kc = 0; kc < it.nkc; ++kc) {
+                for (int kc = 0; kc < it.nkc * kSubPerChunk; ++kc) {
                     if (!mbar_wait(bar(FULL + stage), phase, abort_flag)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
                     const uint32_t sb = base + stage * kStageBytes;
-                    const uint64_t ar = sdesc_sw128(sb);
-                    const uint64_t ai = sdesc_sw128(sb + kTileBytes);
-                    // 256-row B operand [Xr_j ; Xi_j]: two adjacent 16 KiB tiles
-                    const uint64_t b = diag ? ar : sdesc_sw128(sb + 2 * kTileBytes);
+                    const uint64_t ar = sdesc(sb);
+                    const uint64_t ai = sdesc(sb + kTileBytes);
+                    // 256-row B operand [Xr_j ; Xi_j]: two adjacent tiles
+                    const uint64_t b = diag ? ar : sdesc(sb + 2 * kTileBytes);
 #pragma unroll
                     for (int kk = 0; kk < kKc / 32; ++kk) {
                         const uint64_t o = (uint64_t)((kk * 32) >> 4);   // 32-byte K step
@@ -263,9 +287,13 @@ __global__ void __launch_bounds__(192, 1)
         }
     } else {
         // ------------------------------------------------------------ epilogue
-        const int q = warp & 3;                      // TMEM lanes 32q .. 32q+31
-        const int m = q * 32 + lane;                 // tile row
-        const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
+        // Eight warps: TMEM lane quadrant warp % 4, column half (warp - 2) / 4.
+        // Each warp reads its 64 columns 16 at a time and adds them into the
+        // cube; TMEM is released once every warp has read its last chunk.
+        const int q = warp & 3;
+        const int col0 = kEpiCols * ((warp - 2) >> 2);
+        const int m = q * 32 + lane;
+        const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col0;
         uint32_t acc_phase = 0;
         for (int64_t w = blockIdx.x; w < args.nwork; w += gridDim.x) {
             const Item it = get_item(args, &tmap, w);
@@ -277,38 +305,35 @@ __global__ void __launch_bounds__(192, 1)
             tc_fence_after();
             const size_t tb = ((size_t)it.c * it.ntiles + it.t) * (size_t)(2 * kTile * kTile);
 #pragma unroll 1
-            for (int n0 = 0; n0 < kTile; n0 += 16) {
+            for (int n0 = 0; n0 < kEpiCols; n0 += 16) {
                 uint32_t r[4][16];   // R1, P2, P1, R2
                 tmem_ld4_x16(trow + n0, trow + 128 + n0, trow + 256 + n0, trow + 384 + n0, r);
-                if (n0 == kTile - 16) {              // all of this tile's TMEM is read
+                if (n0 == kEpiCols - 16) {           // this warp's TMEM reads are done
                     tc_fence_before();
                     mbar_arrive(bar(ACCE));
                 }
-                const size_t e0 = tb + (size_t)n0 * kTile + m;
+                const size_t e0 = tb + (size_t)(col0 + n0) * kTile + m;
                 if (it.mode == MIXER_VIS_ACC_I64) {
-                    unsigned long long* v = reinterpret_cast<unsigned long long*>(it.vis);
+                    unsigned long long* v = reinterpret_cast<unsigned long long*>(it.vis) + e0;
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
-                        const int32_t vr = (int32_t)(r[0][e] + r[3][e]);
-                        const int32_t vi = (int32_t)(r[2][e] - r[1][e]);
-                        atomicAdd(v + e0 + (size_t)e * kTile, (unsigned long long)(long long)vr);
-                        atomicAdd(v + e0 + (size_t)e * kTile + kTile * kTile,
-                                  (unsigned long long)(long long)vi);
+                        atomicAdd(v + e * kTile, (unsigned long long)(long long)(int32_t)(r[0][e] + r[3][e]));
+                        atomicAdd(v + e * kTile + kTile * kTile,
+                                  (unsigned long long)(long long)(int32_t)(r[2][e] - r[1][e]));
                     }
                 } else if (it.mode == MIXER_VIS_ACC_I32) {
-                    int* v = reinterpret_cast<int*>(it.vis);
+                    int* v = reinterpret_cast<int*>(it.vis) + e0;
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
-                        atomicAdd(v + e0 + (size_t)e * kTile, (int)(r[0][e] + r[3][e]));
-                        atomicAdd(v + e0 + (size_t)e * kTile + kTile * kTile,
-                                  (int)(r[2][e] - r[1][e]));
+                        atomicAdd(v + e * kTile, (int)(r[0][e] + r[3][e]));
+                        atomicAdd(v + e * kTile + kTile * kTile, (int)(r[2][e] - r[1][e]));
                     }
                 } else {
-                    int* v = reinterpret_cast<int*>(it.vis);
+                    int* v = reinterpret_cast<int*>(it.vis) + e0;
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {
-                        v[e0 + (size_t)e * kTile] = (int)(r[0][e] + r[3][e]);
-                        v[e0 + (size_t)e * kTile + kTile * kTile] = (int)(r[2][e] - r[1][e]);
+                        v[e * kTile] = (int)(r[0][e] + r[3][e]);
+                        v[e * kTile + kTile * kTile] = (int)(r[2][e] - r[1][e]);
                     }
                 }
             }
@@ -363,7 +388,8 @@ int xcorr_encode_map(CUtensorMap* map, const int8_t* planes, int32_t nant, int32
     const cuuint32_t box[4] = {kKc, kTile, 1, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<int8_t*>(planes), dims,
-                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     kKc == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? MIXER_OK : MIXER_EINVAL;
 }
@@ -396,7 +422,7 @@ static int xcorr_launch(const int8_t* planes, int32_t nant, int32_t nch, int64_t
     a.nblk = (nant + kTile - 1) / kTile;
     a.ntiles = a.nblk * (a.nblk + 1) / 2;
     a.kbeg = (int32_t)kbeg;
-    a.nkc = (int32_t)((klen + kKc - 1) / kKc);
+    a.nkc = (int32_t)((klen + kWorkChunk - 1) / kWorkChunk);
     a.mode = mode;
     a.pad_ = 0;
     a.nwork = (int64_t)nch * a.ntiles;
@@ -406,7 +432,7 @@ static int xcorr_launch(const int8_t* planes, int32_t nant, int32_t nch, int64_t
     a.probs = nullptr;
     a.work = nullptr;
     const int64_t grid = a.nwork < sm_count() ? a.nwork : sm_count();
-    k_xcorr_tri<<<(unsigned)grid, 192, kSmemBytes, st>>>(map, a);
+    k_xcorr_tri<<<(unsigned)grid, kThreads, kSmemBytes, st>>>(map, a);
     MIXER_CK(cudaGetLastError());
     return MIXER_OK;
 }
@@ -426,7 +452,7 @@ int xcorr_launch_table(const CUtensorMap* d_tmaps, const XcorrProblem* d_probs,
     a.work = d_work;
     CUtensorMap unused;
     memset(&unused, 0, sizeof(unused));
-    k_xcorr_tri<<<(unsigned)(grid < nwork ? grid : nwork), 192, kSmemBytes, st>>>(unused, a);
+    k_xcorr_tri<<<(unsigned)(grid < nwork ? grid : nwork), kThreads, kSmemBytes, st>>>(unused, a);
     MIXER_CK(cudaGetLastError());
     return MIXER_OK;
 }
