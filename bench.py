@@ -43,11 +43,34 @@ L2_BYTES = 126 * 1024 * 1024
 XCORR_TRAFFIC_RATIO = 1.6957 / 1.7456
 
 
-def configure(nch):
-    """Channel count of the packets; the payload stays 8192 bytes (2 x nch x tpkt)."""
-    global NCH, TPKT, STRIDE, HEAPS_PER_SUB
-    if 4096 % nch or (4096 // nch) % 16:
-        raise SystemExit("--nch must divide 4096 with 4096/nch a multiple of 16")
+# The plain (one array) workloads.  nch x tpkt = 4096 keeps the 8192-byte payload.
+PLAIN_CONFIGS = {
+    # the reference's own array: 16 x 16, 128 ch, K 256, 64 sub-integrations per dump,
+    # star A1 6 at (0.10, -0.05) + planet 1.5 c/128 at radius 0.2, noise sigma 16
+    "small": dict(nant=256, side=16, nch=128, ksub=256, grid=32, sigma=16.0, noise=0, batch=64,
+                  text="filled 16x16=256 elements, 128 ch, K=256, 64 sub-integrations per dump "
+                       "(one step = one dump), star + planet + sigma 16 noise"),
+    # the larger plain array (the headline)
+    "plain": dict(nant=1024, side=32, nch=256, ksub=1024, grid=64, sigma=8.0, noise=0, batch=8,
+                  text="plain array 32x32=1024 elements, 256 ch, K=1024 per sub-integration, "
+                       "3 sources + sigma 8 noise, int64 integration"),
+    # large-N stress: uniform int8 in [-127, 127], 128 x 128 imaging
+    "large": dict(nant=4096, side=64, nch=64, ksub=2048, grid=128, sigma=0.0, noise=1, batch=8,
+                  text="large-N stress 64x64=4096 elements, 64 ch, K=2048 per sub-integration, "
+                       "uniform int8 in [-127, 127], int64 integration, 128x128 imaging"),
+}
+CFG = PLAIN_CONFIGS["plain"]
+
+
+def configure(nch=None, name="plain"):
+    """Select a plain workload; optionally override the channel count of the
+    packets (the payload stays 8192 bytes: tpkt = 4096 / nch)."""
+    global CFG, NANT, SIDE, NCH, TPKT, KSUB, G, SIGMA, STRIDE, HEAPS_PER_SUB
+    CFG = PLAIN_CONFIGS[name]
+    NANT, SIDE, KSUB, G, SIGMA = CFG["nant"], CFG["side"], CFG["ksub"], CFG["grid"], CFG["sigma"]
+    nch = nch or CFG["nch"]
+    if 4096 % nch or (4096 // nch) % 16 or KSUB % (4096 // nch):
+        raise SystemExit("--nch must divide 4096 with 4096/nch a multiple of 16 dividing K")
     NCH, TPKT = nch, 4096 // nch
     STRIDE = HDR + 2 * NCH * TPKT
     HEAPS_PER_SUB = KSUB // TPKT
@@ -55,6 +78,10 @@ def configure(nch):
 
 def sources(seed=SEED):
     import numpy as np
+    if CFG is PLAIN_CONFIGS["small"]:
+        return [(0.10, -0.05, 6.0, 0.0), (0.2, 0.0, 0.0, 1.5)]
+    if CFG["noise"] == 1:
+        return []
     rng = np.random.default_rng(seed)
     lm = rng.uniform(-0.4, 0.4, size=(3, 2))
     return [(float(lm[s, 0]), float(lm[s, 1]), amp, 0.0) for s, amp in enumerate((4.0, 2.0, 1.0))]
@@ -176,16 +203,18 @@ def measured_peaks():
 
 
 def make_packets(mixer, torch, dev, nheaps, heap0=0):
-    sky = torch.from_numpy(mixer.sky_table(NANT, NCH, SIDE, sources())).to(dev)
+    src = sources()
+    sky = torch.from_numpy(mixer.sky_table(NANT, NCH, SIDE, src)).to(dev) if src else None
     pk = torch.empty(nheaps * NANT * STRIDE, dtype=torch.uint8, device=dev)
     mixer.gen_packets(pk, STRIDE, HDR, NANT, NCH, TPKT, nheaps, heap0, heap0 * NANT, 4096, sky,
-                      SIGMA, SEED, 0)
+                      SIGMA, SEED, CFG["noise"])
     return pk
 
 
-def cpu_correlator_sample(packets_host, nheaps, target_s=12.0, max_threads=0):
+def cpu_correlator_sample(packets_host, nheaps, target_s=12.0, max_threads=0, max_out=2e9):
     """Time the oracle's OpenMP int64 correlator on a channel subset of one
-    sub-integration; returns (gbps_equivalent, cores, sample_description)."""
+    sub-integration; returns (gbps_equivalent, cores, sample_description,
+    seconds, full-square int64 V of the sampled channels)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     import oracle
@@ -198,7 +227,7 @@ def cpu_correlator_sample(packets_host, nheaps, target_s=12.0, max_threads=0):
     t0 = time.perf_counter()
     oracle.correlate(planes, c0=0, nc=1, out=out, mirror=False)
     t1 = time.perf_counter() - t0
-    nc = int(max(1, min(NCH, target_s / max(t1, 1e-3))))
+    nc = int(max(1, min(NCH, target_s / max(t1, 1e-3), max_out / (16.0 * NANT * NANT))))
     out = np.zeros((nc, 2, NANT, NANT), dtype=np.int64)
     t0 = time.perf_counter()
     oracle.correlate(planes, c0=0, nc=nc, out=out, mirror=False)
@@ -207,7 +236,7 @@ def cpu_correlator_sample(packets_host, nheaps, target_s=12.0, max_threads=0):
     gbps = wire_gbps(HEAPS_PER_SUB * NANT * frac, dt)
     desc = (f"OpenMP int64 correlator on {nc}/{NCH} channels of one K={KSUB} sub-integration "
             f"({NANT} elements, lower triangle), {dt:.2f} s; Gb/s scaled by channel fraction")
-    return gbps, cores, desc, dt
+    return gbps, cores, desc, dt, out
 
 
 def run_reference(args):
@@ -218,8 +247,10 @@ def run_reference(args):
         return 0
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    sky = oracle.sky_table(NANT, NCH, SIDE, sources())
-    pk = oracle.gen_packets(NANT, NCH, TPKT, HEAPS_PER_SUB, sky=sky, sigma=SIGMA, seed=SEED)
+    src = sources()
+    sky = oracle.sky_table(NANT, NCH, SIDE, src) if src else None
+    pk = oracle.gen_packets(NANT, NCH, TPKT, HEAPS_PER_SUB, sky=sky, sigma=SIGMA, seed=SEED,
+                            mode=CFG["noise"])
     planes = oracle.corner_turn(pk, NANT, NCH, TPKT, HEAPS_PER_SUB)
     cores = oracle.max_threads()
     nc = args.ref_channels
@@ -239,8 +270,7 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int8->int64", "data": "synthetic (seeded packet source)",
-        "config": {"workload": "plain array 32x32=1024 elements, 256 ch, K=1024, 3 sources + "
-                   "sigma 8 noise", "nant": NANT, "nch": NCH, "ksub": KSUB,
+        "config": {"workload": CFG["text"], "nant": NANT, "nch": NCH, "ksub": KSUB,
                    "sample": f"{nc} of {NCH} channels per step"},
         "tops": tri_ops(KSUB) * frac * args.steps / tot / 1e12,
         "cpu_baseline": {"value": value, "unit": "Gb/s", "cores": cores, "kind": "port",
@@ -712,8 +742,7 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int8->int32(TMEM)->int64",
         "data": "synthetic (seeded packet source, wire format)",
-        "config": {"workload": "plain array 32x32=1024 elements, 256 ch, K=1024 per "
-                   "sub-integration, 3 sources + sigma 8 noise, int64 integration",
+        "config": {"workload": CFG["text"],
                    "nant": NANT, "nch": NCH, "tpkt": TPKT, "ksub": KSUB,
                    "subints_per_step": S, "packets_per_step": npk,
                    "bytes_per_step": npk * STRIDE,
@@ -737,11 +766,38 @@ def run_ours(args):
         "gpu_launches": 2 * args.steps,
         "e2e": e2e,
     }
-    if rank == 0 and not args.no_cpu_baseline:
-        hp = host[: HEAPS_PER_SUB * NANT * STRIDE].numpy()
-        gbps, cores, desc, _ = cpu_correlator_sample(hp, HEAPS_PER_SUB, target_s=args.cpu_seconds)
-        line["cpu_baseline"] = {"value": gbps, "unit": "Gb/s", "cores": cores, "kind": "port",
-                                "sample": desc}
+    # ---- imaging of the integrated cube (grid + FFT), device resident ------------
+    with mixer.ArrayContext(nant=NANT, nch=NCH, tpkt=TPKT, ksub=KSUB, nsub_dump=1, side_x=SIDE,
+                            grid=G, pkt_stride=STRIDE, hdr_bytes=HDR, max_heaps=HEAPS_PER_SUB) as ic:
+        ic.correlate(pk, HEAPS_PER_SUB, seq0=0)
+        dimg = torch.empty(NCH * G * G, dtype=torch.float32, device=dev)
+        ic.image(dimg)
+        torch.cuda.synchronize()
+        i0, i1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        i0.record(stream)
+        for _ in range(10):
+            ic.image(dimg)
+        i1.record(stream)
+        torch.cuda.synchronize()
+        line["image_ms"] = i0.elapsed_time(i1) / 10
+        line["image_grid"] = G
+        if rank == 0 and not args.no_cpu_baseline:
+            # CPU baseline (the oracle's OpenMP correlator on a channel subset of the first
+            # sub-integration); its output also checks the GPU's V for that sub-integration
+            hp = host[: HEAPS_PER_SUB * NANT * STRIDE].numpy()
+            gbps, cores, desc, _, ref = cpu_correlator_sample(hp, HEAPS_PER_SUB,
+                                                              target_s=args.cpu_seconds)
+            line["cpu_baseline"] = {"value": gbps, "unit": "Gb/s", "cores": cores, "kind": "port",
+                                    "sample": desc}
+            ncheck = min(4, ref.shape[0])
+            got = torch.empty(ncheck * 2 * NANT * NANT, dtype=torch.int64, device=dev)
+            mixer.vis_unpack_i64(ic.state_ptr(), NANT, ncheck, got)
+            torch.cuda.synchronize()
+            import numpy as np
+            line["bit_exact_vs_cpu"] = {
+                "channels": ncheck, "subints": 1,
+                "equal": bool(np.array_equal(got.cpu().numpy().reshape(ncheck, 2, NANT, NANT),
+                                             ref[:ncheck]))}
     if rank == 0:
         print(json.dumps(line))
     if pg is not None:
@@ -755,18 +811,23 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=8, help="sub-integrations per step")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="sub-integrations per step (0: the workload's default)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--e2e-chunk", type=int, default=2, help="sub-integrations per H2D chunk")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-channels", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--nch", type=int, default=256, help="channels per packet (tpkt = 4096/nch)")
+    ap.add_argument("--nch", type=int, default=0,
+                    help="channels per packet, tpkt = 4096/nch (0: the workload's)")
     ap.add_argument("--serve-seconds", type=float, default=20.0)
     ap.add_argument("--serve-gbps", type=float, default=380.0)
     ap.add_argument("--serve-budget-gb", type=float, default=6.0)
-    ap.add_argument("--config", default="plain", choices=["plain", "batched", "serve"],
-                    help="plain: the 1024-element array (headline); batched: 48 uneven arrays")
+    ap.add_argument("--config", default="plain",
+                    choices=["plain", "small", "large", "batched", "serve"],
+                    help="plain: the 1024-element array (headline); small: the reference's "
+                         "256-element array; large: 4096 elements; batched: 48 uneven arrays; "
+                         "serve: 8 concurrent streams")
     ap.add_argument("--small-arrays", action="store_true",
                     help="batched config with arrays too small to fill the GPU alone")
     ap.add_argument("--sweep-quick", action="store_true", help="fewer sweep points")
@@ -775,7 +836,9 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="device-resident steps only (small case for ncu captures)")
     args = ap.parse_args()
-    configure(args.nch)
+    configure(args.nch, args.config if args.config in PLAIN_CONFIGS else "plain")
+    if args.batch <= 0:
+        args.batch = CFG["batch"]
     if args.warmup < 3 and args.impl == "ours" and not args.profile:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "reference":
