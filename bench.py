@@ -529,11 +529,13 @@ def run_serve(args):
             nxt = time.perf_counter()
             ta = nxt
             j = 0
+            own = torch.cuda.Stream()
             while time.perf_counter() - t0 < stops[i]:
                 if j % nsub == 0:                      # new lap over the pool: re-stamp seqs
-                    torch.cuda.synchronize()
-                    mixer.restamp_seq(pools[i], nsub * hps * nant, stride, j * hps * nant)
-                    torch.cuda.synchronize()
+                    srv.sync_copies()                  # the previous lap has been copied
+                    mixer.restamp_seq(pools[i], nsub * hps * nant, stride, j * hps * nant,
+                                      stream=own)
+                    own.synchronize()
                 if interval > 0:
                     while time.perf_counter() < nxt:
                         time.sleep(min(0.0005, max(0.0, nxt - time.perf_counter())))
@@ -848,7 +850,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nch", type=int, default=0,
                     help="channels per packet, tpkt = 4096/nch (0: the workload's)")
-    ap.add_argument("--serve-seconds", type=float, default=20.0)
+    ap.add_argument("--serve-seconds", type=float, default=30.0)
     ap.add_argument("--serve-gbps", type=float, default=380.0)
     ap.add_argument("--serve-budget-gb", type=float, default=6.0)
     ap.add_argument("--config", default="plain",

@@ -613,3 +613,9 @@ extern "C" int mixer_server_stats(mixer_server* sv, mixer_server_counters* st) {
     st->seq_errors = se;
     return sv->error.load() ? sv->error.load() : (ke ? MIXER_ETIMEOUT : MIXER_OK);
 }
+
+extern "C" int mixer_server_sync_copies(mixer_server* sv) {
+    if (!sv) return MIXER_EINVAL;
+    MIXER_CK(cudaStreamSynchronize(sv->copy));
+    return MIXER_OK;
+}

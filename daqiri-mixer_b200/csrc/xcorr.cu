@@ -19,13 +19,15 @@
 // through 4-D TMA tensor loads (128-byte swizzle, 128 x 128-byte boxes)
 // into a 3-deep shared-memory ring.  One elected thread issues all
 // tcgen05.mma; the int32 accumulators stay in TMEM for the whole K range of
-// the launch; four epilogue warps read them back with tcgen05.ld and add
+// the launch; eight epilogue warps read them back with tcgen05.ld and add
 // them into the tile-packed int32 or int64 cube in HBM.
 //
-// Warp roles (192 threads, one CTA per SM, persistent over work items):
+// Warp roles (320 threads with the default build, one CTA per SM, persistent
+// over work items):
 //   warp 0      TMA producer
 //   warp 1      TMEM allocator + MMA issuer
-//   warps 2..5  epilogue (TMEM lane quadrant = warp % 4)
+//   warps 2..9  epilogue (TMEM lane quadrant = warp % 4, 64-column half =
+//               (warp - 2) / 4)
 #include "common.cuh"
 #include "xcorr.cuh"
 #include <cstring>

@@ -134,6 +134,7 @@ _sig("mixer_server_close", C.c_int, _vp, _i32)
 _sig("mixer_server_submit", C.c_int, _vp, _i32, _vp, _i64, _u32, _i32)
 _sig("mixer_server_poll", C.c_int, _vp, _i32, C.POINTER(DumpInfo), _vp)
 _sig("mixer_server_stats", C.c_int, _vp, C.POINTER(ServerCounters))
+_sig("mixer_server_sync_copies", C.c_int, _vp)
 _sig("mixer_create", C.c_int, C.POINTER(ArrayDesc), C.POINTER(_vp))
 _sig("mixer_destroy", C.c_int, _vp)
 _sig("mixer_reset", C.c_int, _vp, _vp)
@@ -163,6 +164,7 @@ EXPORTED = [
     "mixer_batch_capture_graph", "mixer_batch_replay", "mixer_batch_info", "mixer_batch_destroy",
     "mixer_server_create", "mixer_server_destroy", "mixer_server_stream_bytes", "mixer_server_open",
     "mixer_server_close", "mixer_server_submit", "mixer_server_poll", "mixer_server_stats",
+    "mixer_server_sync_copies",
     "mixer_restamp_seq", "mixer_ctx_shape", "mixer_write_vis_i64", "mixer_state_save",
     "mixer_state_load", "mixer_align_heaps",
 ]
@@ -475,6 +477,9 @@ class Server:
             return False
         _check(rc, "mixer_server_submit")
         return True
+
+    def sync_copies(self):
+        _check(_lib.mixer_server_sync_copies(self._h), "mixer_server_sync_copies")
 
     def poll(self, sid, out=None):
         info = DumpInfo()

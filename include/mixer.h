@@ -343,6 +343,9 @@ int mixer_server_submit(mixer_server* sv, int32_t stream_id, const void* packets
 /* Oldest completed dump of the stream, copied to `out` (host, may be NULL to
  * discard) and released; info->available = 0 when none is ready. */
 int mixer_server_poll(mixer_server* sv, int32_t stream_id, mixer_dump_info* info, float* out);
+/* Waits until every heap submitted so far (all streams) has been copied into
+ * the server's staging rings, so the caller may reuse its packet buffers. */
+int mixer_server_sync_copies(mixer_server* sv);
 /* Counters and p50 / p99 dump latency over all dumps so far. */
 int mixer_server_stats(mixer_server* sv, mixer_server_counters* st);
 
