@@ -411,8 +411,10 @@ static int set_smem_attr() {
 int xcorr_sm_count() { return sm_count(); }
 
 // Launch over samples [kbeg, kbeg + klen) with klen <= MIXER_KMAX_I32.
+// At most max_ctas persistent CTAs (<= 0: one per SM).
 static int xcorr_launch(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt, int64_t kbeg,
-                        int64_t klen, int32_t mode, void* vis, int32_t* err, cudaStream_t st) {
+                        int64_t klen, int32_t mode, void* vis, int32_t max_ctas, int32_t* err,
+                        cudaStream_t st) {
     CUtensorMap map;
     int rc = xcorr_encode_map(&map, planes, nant, nch, kt, kbeg + klen);
     if (rc != MIXER_OK) return rc;
@@ -433,7 +435,9 @@ static int xcorr_launch(const int8_t* planes, int32_t nant, int32_t nch, int64_t
     a.tmaps = nullptr;
     a.probs = nullptr;
     a.work = nullptr;
-    const int64_t grid = a.nwork < sm_count() ? a.nwork : sm_count();
+    int64_t grid = sm_count();
+    if (max_ctas > 0 && max_ctas < grid) grid = max_ctas;
+    if (a.nwork < grid) grid = a.nwork;
     k_xcorr_tri<<<(unsigned)grid, kThreads, kSmemBytes, st>>>(map, a);
     MIXER_CK(cudaGetLastError());
     return MIXER_OK;
@@ -472,9 +476,9 @@ extern "C" int64_t mixer_vis_elems(int32_t nant, int32_t nch) {
     return (int64_t)nch * mixer_vis_tiles(nant) * 2 * 128 * 128;
 }
 
-extern "C" int mixer_xcorr_tri(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt,
-                               int64_t kbeg, int64_t klen, int32_t mode, void* vis, int32_t* err,
-                               void* stream) {
+extern "C" int mixer_xcorr_tri_ex(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt,
+                                  int64_t kbeg, int64_t klen, int32_t mode, void* vis,
+                                  int32_t max_ctas, int32_t* err, void* stream) {
     if (!planes || !vis || nant <= 0 || nch <= 0 || kt <= 0 || kt % 16 != 0) return MIXER_EINVAL;
     if (kbeg < 0 || kbeg % 16 != 0 || klen <= 0 || kbeg + klen > kt) return MIXER_EINVAL;
     if (mode != MIXER_VIS_STORE_I32 && mode != MIXER_VIS_ACC_I32 && mode != MIXER_VIS_ACC_I64)
@@ -484,12 +488,19 @@ extern "C" int mixer_xcorr_tri(const int8_t* planes, int32_t nant, int32_t nch, 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (mode != MIXER_VIS_ACC_I64) {
         if (klen > MIXER_KMAX_I32) return MIXER_EOVERFLOW;
-        return mixer::xcorr_launch(planes, nant, nch, kt, kbeg, klen, mode, vis, err, st);
+        return mixer::xcorr_launch(planes, nant, nch, kt, kbeg, klen, mode, vis, max_ctas, err, st);
     }
     for (int64_t k = 0; k < klen; k += MIXER_KMAX_I32) {
         const int64_t len = (klen - k) < MIXER_KMAX_I32 ? (klen - k) : MIXER_KMAX_I32;
-        const int rc = mixer::xcorr_launch(planes, nant, nch, kt, kbeg + k, len, mode, vis, err, st);
+        const int rc =
+            mixer::xcorr_launch(planes, nant, nch, kt, kbeg + k, len, mode, vis, max_ctas, err, st);
         if (rc != MIXER_OK) return rc;
     }
     return MIXER_OK;
+}
+
+extern "C" int mixer_xcorr_tri(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt,
+                               int64_t kbeg, int64_t klen, int32_t mode, void* vis, int32_t* err,
+                               void* stream) {
+    return mixer_xcorr_tri_ex(planes, nant, nch, kt, kbeg, klen, mode, vis, 0, err, stream);
 }

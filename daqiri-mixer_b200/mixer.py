@@ -100,6 +100,7 @@ _sig("mixer_vis_elems", _i64, _i32, _i32)
 _sig("mixer_corner_turn", C.c_int, _vp, _i64, _i32, _i32, _i32, _i32, _i32, _u32, _vp, _i64, _i64,
      _vp, _vp, _vp)
 _sig("mixer_xcorr_tri", C.c_int, _vp, _i32, _i32, _i64, _i64, _i64, _i32, _vp, _vp, _vp)
+_sig("mixer_xcorr_tri_ex", C.c_int, _vp, _i32, _i32, _i64, _i64, _i64, _i32, _vp, _i32, _vp, _vp)
 _sig("mixer_vis_flush", C.c_int, _vp, _vp, _i64, _vp)
 _sig("mixer_vis_dump_f32", C.c_int, _vp, _i32, _i32, _vp, _vp)
 _sig("mixer_vis_unpack_i64", C.c_int, _vp, _i32, _i32, _vp, _vp)
@@ -153,7 +154,7 @@ _sig("mixer_shm_close", C.c_int, _vp, _i32)
 
 EXPORTED = [
     "mixer_vis_tiles", "mixer_vis_elems", "mixer_strerror", "mixer_device_ok",
-    "mixer_corner_turn", "mixer_xcorr_tri", "mixer_vis_flush", "mixer_vis_dump_f32",
+    "mixer_corner_turn", "mixer_xcorr_tri", "mixer_xcorr_tri_ex", "mixer_vis_flush", "mixer_vis_dump_f32",
     "mixer_vis_unpack_i64", "mixer_grid", "mixer_image_fft", "mixer_image_noalloc",
     "mixer_sky_table",
     "mixer_gen_packets", "mixer_desc_default", "mixer_create", "mixer_destroy", "mixer_reset",
@@ -222,7 +223,11 @@ def corner_turn(packets, pkt_stride, hdr_bytes, nant, nch, tpkt, nheaps, seq0, p
                                   _ptr(err), _stream(stream)), "mixer_corner_turn")
 
 
-def xcorr_tri(planes, nant, nch, kt, kbeg, klen, mode, vis, err=None, stream=None):
+def xcorr_tri(planes, nant, nch, kt, kbeg, klen, mode, vis, err=None, stream=None, max_ctas=0):
+    if max_ctas:
+        _check(_lib.mixer_xcorr_tri_ex(_ptr(planes), nant, nch, kt, kbeg, klen, mode, _ptr(vis),
+                                       max_ctas, _ptr(err), _stream(stream)), "mixer_xcorr_tri_ex")
+        return
     _check(_lib.mixer_xcorr_tri(_ptr(planes), nant, nch, kt, kbeg, klen, mode, _ptr(vis), _ptr(err),
                                 _stream(stream)), "mixer_xcorr_tri")
 

@@ -105,6 +105,13 @@ int mixer_xcorr_tri(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt,
                     int64_t kbeg, int64_t klen, int32_t mode, void* vis,
                     int32_t* err, void* stream);
 
+/* Same, with at most max_ctas persistent CTAs (<= 0: one per SM).  Leaving
+ * SMs free lets an HBM-bound kernel on another stream (the next corner-turn)
+ * run beside the tensor-bound GEMM. */
+int mixer_xcorr_tri_ex(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt,
+                       int64_t kbeg, int64_t klen, int32_t mode, void* vis,
+                       int32_t max_ctas, int32_t* err, void* stream);
+
 /* int32 -> int64 integration: vis64 += vis32; vis32 = 0 over n elements.
  * Replaces k_flush_cube (src/rx_host_corr.cu:90-95), which promotes into a
  * float cube and loses exactness past 2^24. */

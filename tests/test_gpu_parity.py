@@ -148,6 +148,23 @@ def test_xcorr_accumulate_modes(cuda):
     assert int(v32.abs().max().item()) == 0
 
 
+@pytest.mark.parametrize("max_ctas", [1, 7, 100000])
+def test_xcorr_cta_cap_is_exact(cuda, max_ctas):
+    """mixer_xcorr_tri_ex: fewer persistent CTAs walk more items each, same cube."""
+    import torch
+    rng = np.random.default_rng(31 + max_ctas)
+    nant, nch, kt = 384, 3, 512
+    planes = _rand_planes(rng, nch, nant, kt)
+    v64 = _zeros(mixer.vis_elems(nant, nch), torch.int64, cuda)
+    err = _zeros(1, torch.int32, cuda)
+    mixer.xcorr_tri(_t(planes, cuda), nant, nch, kt, 0, kt, mixer.VIS_ACC_I64, v64, err,
+                    max_ctas=max_ctas)
+    _sync()
+    assert int(err.item()) == 0
+    ref = oracle.vis_tile_pack(oracle.correlate(planes)).reshape(-1)
+    assert np.array_equal(v64.cpu().numpy(), ref)
+
+
 def test_xcorr_extreme_inputs(cuda):
     """-128 everywhere: exact here; the reference's -A_im (src/cgemm.cuh:52) wraps."""
     import torch
