@@ -220,8 +220,11 @@ int mixer_batch_create(const mixer_xcorr_problem* probs, int32_t nprob, mixer_ba
  * index 0..nclass-1) and item order. */
 int mixer_batch_plan(mixer_batch* b, const int32_t* split_per_class, int32_t nclass, int32_t order);
 /* Autotuner: times candidate plans (order x greedy per-class K-split) on the
- * caller's own buffers with `reps` launches each and keeps the fastest.  The
- * ACC-mode cubes accumulate every trial: zero them afterwards. */
+ * caller's own buffers, `reps` launches per sample, each candidate against the
+ * incumbent in an A-B-B-A pairing (clock drift cancels); a change is kept only
+ * when it is at least 2 % faster, and the result must beat the default plan
+ * (longest-first, no split) by as much or the default is kept.  The ACC-mode
+ * cubes accumulate every trial: zero them afterwards. */
 int mixer_batch_autotune(mixer_batch* b, int32_t reps, void* stream, float* best_ms);
 /* One launch of the current plan. */
 int mixer_batch_run(mixer_batch* b, void* stream);
