@@ -61,6 +61,30 @@ __global__ void __launch_bounds__(256)
     const int V = hg * tpkt / 16;              // 16-byte vectors per (plane, channel) row
     const int total = 2 * nchg * V;
     const int64_t kcol = k0 + (int64_t)g * hg * tpkt;
+    if (blockDim.x % V == 0) {
+        // Each thread keeps one column v of the rows and steps over (plane,
+        // channel) rows with additions only.
+        const int v = threadIdx.x % V;
+        const int rstep = blockDim.x / V;
+        const int kb = v * 16;
+        const int hl = kb / tpkt;
+        const uint8_t* srow = sm + hl * hstride + (kb - hl * tpkt);
+        int8_t* dcol = planes + (int64_t)a * kt + kcol + kb;
+        const int64_t cstride = (int64_t)nant * kt;   // one channel row to the next
+        int pc = threadIdx.x / V;
+        int plane = pc / nchg;
+        int cl = pc - plane * nchg;
+        for (; pc < 2 * nchg; pc += rstep) {
+            const uint4 val = *reinterpret_cast<const uint4*>(srow + plane * part + cl * tpkt);
+            *reinterpret_cast<uint4*>(dcol + ((int64_t)plane * nch + c0 + cl) * cstride) = val;
+            cl += rstep;
+            while (cl >= nchg) {
+                cl -= nchg;
+                ++plane;
+            }
+        }
+        return;
+    }
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
         const int v = idx % V;
         const int pc = idx / V;                // plane * nchg + local channel
