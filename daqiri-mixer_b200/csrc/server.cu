@@ -27,6 +27,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -45,7 +46,7 @@ constexpr int kDumpSlots = 2;
 
 struct DumpSlot {
     float* host = nullptr;          // pinned FP32 cube
-    int state = 0;                  // 0 free, 1 in flight, 2 ready
+    int state = 0;                  // 0 free, 1 in flight, 2 ready, 3 being read by poll
     int64_t index = 0;
     double t_last_submit = 0.0;
     std::atomic<double> t_done{0.0};
@@ -81,6 +82,7 @@ struct Stream {
     int64_t dumps_emitted = 0;
     int64_t dumps_dropped = 0;
     int64_t bytes_in = 0;
+    int readers = 0;                // mixer_server_poll copies in progress
     uint32_t seq_next = 0;
     bool seq_set = false;
 };
@@ -115,6 +117,13 @@ struct mixer_server {
     bool table_used[2] = {false, false};
     int tsel = 0;
     int32_t* d_err = nullptr;
+    // Stream state comes from a server-owned stream-ordered pool and pinned dump
+    // buffers are recycled, so opening or closing a stream never runs the
+    // device-wide synchronisation of cudaMalloc / cudaFree / cudaFreeHost while
+    // other streams are being served.
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t alloc = nullptr;
+    std::multimap<size_t, float*> pinned_cache;   // guarded by mu
     std::thread worker;
     std::atomic<bool> stop{false};
     std::atomic<int> error{0};
@@ -141,17 +150,18 @@ int64_t stream_bytes(const mixer_array_desc& d, int64_t ring_subs, int64_t batch
     return ring + planes + vis + dump + 4096;
 }
 
-void free_stream(Stream& s) {
-    cudaFree(s.ring);
-    cudaFree(s.planes);
-    cudaFree(s.vis);
-    cudaFree(s.dump_dev);
-    cudaFree(s.d_seq_err);
+// Caller holds sv->mu; the stream's GPU work has finished.
+void free_stream(mixer_server* sv, Stream& s) {
+    for (void* p : {(void*)s.ring, (void*)s.planes, (void*)s.vis, (void*)s.dump_dev,
+                    (void*)s.d_seq_err})
+        if (p) cudaFreeAsync(p, sv->alloc);
     for (auto e : s.ev_ready) cudaEventDestroy(e);
     for (auto e : s.ev_free) cudaEventDestroy(e);
     if (s.ev_dump_copied) cudaEventDestroy(s.ev_dump_copied);
     if (s.ev_dump_kernel) cudaEventDestroy(s.ev_dump_kernel);
-    for (auto& d : s.dump) cudaFreeHost(d.host);
+    const size_t dump_bytes = (size_t)s.d.nch * 2 * s.d.nant * s.d.nant * sizeof(float);
+    for (auto& d : s.dump)
+        if (d.host) sv->pinned_cache.emplace(dump_bytes, d.host);
     s.ring = nullptr;
     s.planes = nullptr;
     s.vis = nullptr;
@@ -167,6 +177,7 @@ void free_stream(Stream& s) {
     }
     s.used = false;
     s.closing = false;
+    s.readers = 0;
 }
 
 // One iteration of the continuous-batching loop.  Returns true if it did work.
@@ -210,9 +221,11 @@ bool serve_once(mixer_server* sv) {
             cudaStreamWaitEvent(comp, s.ev_ready[slot + run - 1], 0);   // copies complete in order
             const uint8_t* src = s.ring + slot * s.hps * s.heap_bytes;
             const uint32_t seq = s.seq_next + (uint32_t)(sub * s.hps * s.d.nant);
-            mixer_corner_turn(src, s.d.pkt_stride, s.d.hdr_bytes, s.d.nant, s.d.nch, s.d.tpkt,
-                              (int32_t)(run * s.hps), seq, s.planes, s.kt, q * s.d.ksub, s.d_seq_err,
-                              sv->d_err, comp);
+            const int crc = mixer_corner_turn(src, s.d.pkt_stride, s.d.hdr_bytes, s.d.nant,
+                                              s.d.nch, s.d.tpkt, (int32_t)(run * s.hps), seq,
+                                              s.planes, s.kt, q * s.d.ksub, s.d_seq_err, sv->d_err,
+                                              comp);
+            if (crc != MIXER_OK) sv->error.store(crc);
             for (int64_t u = 0; u < run; ++u) cudaEventRecord(s.ev_free[slot + u], comp);
             q += run;
         }
@@ -221,7 +234,8 @@ bool serve_once(mixer_server* sv) {
         const int64_t klen = ready[r].nsub * s.d.ksub;
         const uint32_t nkc = (uint32_t)((klen + 127) / 128);
         CUtensorMap m;
-        mixer::xcorr_encode_map(&m, s.planes, s.d.nant, s.d.nch, s.kt, klen);
+        const int mrc = mixer::xcorr_encode_map(&m, s.planes, s.d.nant, s.d.nch, s.kt, klen);
+        if (mrc != MIXER_OK) sv->error.store(mrc);
         maps.push_back(m);
         probs.push_back(mixer::XcorrProblem{s.d.nant, s.d.nch, ntiles, 0, MIXER_VIS_ACC_I64, 0, s.vis});
         for (int32_t c = 0; c < s.d.nch; ++c)
@@ -245,11 +259,19 @@ bool serve_once(mixer_server* sv) {
     if ((int64_t)work.size() > sv->work_cap[ts]) {
         cudaFree(sv->d_work[ts]);
         cudaFreeHost(sv->h_work[ts]);
+        sv->d_work[ts] = nullptr;
+        sv->h_work[ts] = nullptr;
+        sv->work_cap[ts] = 0;
         const size_t cap = work.size() + work.size() / 2;
-        cudaMalloc(&sv->d_work[ts], cap * sizeof(mixer::XcorrWork));
-        cudaMallocHost(&sv->h_work[ts], cap * sizeof(mixer::XcorrWork));
+        cudaError_t e = cudaMalloc(&sv->d_work[ts], cap * sizeof(mixer::XcorrWork));
+        if (e == cudaSuccess) e = cudaMallocHost(&sv->h_work[ts], cap * sizeof(mixer::XcorrWork));
+        if (e != cudaSuccess) {
+            sv->error.store(mixer::cuda_status(e, "server work list"));
+            return false;
+        }
         sv->work_cap[ts] = (int64_t)cap;
     }
+    if (sv->error.load()) return false;
     memcpy(sv->h_maps[ts], maps.data(), np * sizeof(CUtensorMap));
     memcpy(sv->h_probs[ts], probs.data(), np * sizeof(mixer::XcorrProblem));
     memcpy(sv->h_work[ts], work.data(), work.size() * sizeof(mixer::XcorrWork));
@@ -281,6 +303,10 @@ bool serve_once(mixer_server* sv) {
                 slot = q;
                 break;
             }
+        if (slot < 0) {                     // cannot happen: checked before the launch
+            sv->error.store(MIXER_EINVAL);
+            continue;
+        }
         DumpSlot& ds = s.dump[slot];
         if (s.dump_copy_pending) cudaStreamWaitEvent(comp, s.ev_dump_copied, 0);
         mixer_vis_dump_f32(s.vis, s.d.nant, s.d.nch, s.dump_dev, comp);
@@ -364,8 +390,21 @@ extern "C" int mixer_server_create(const mixer_server_cfg* cfg, mixer_server** o
     if ((e = cudaGetDevice(&sv->dev)) != cudaSuccess) return fail(e, "cudaGetDevice");
     if ((e = cudaStreamCreateWithFlags(&sv->copy, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&sv->comp, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&sv->d2h, cudaStreamNonBlocking)) != cudaSuccess)
+        (e = cudaStreamCreateWithFlags(&sv->d2h, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&sv->alloc, cudaStreamNonBlocking)) != cudaSuccess)
         return fail(e, "server streams");
+    {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = sv->dev;
+        if ((e = cudaMemPoolCreate(&sv->pool, &props)) != cudaSuccess) return fail(e, "server pool");
+        uint64_t keep = UINT64_MAX;   // freed stream memory stays in the pool for the next open
+        if ((e = cudaMemPoolSetAttribute(sv->pool, cudaMemPoolAttrReleaseThreshold, &keep)) !=
+            cudaSuccess)
+            return fail(e, "server pool");
+    }
     for (int t = 0; t < 2; ++t) {
         if ((e = cudaMalloc(&sv->d_maps[t], cfg->max_streams * sizeof(CUtensorMap))) != cudaSuccess ||
             (e = cudaMalloc(&sv->d_probs[t], cfg->max_streams * sizeof(mixer::XcorrProblem))) != cudaSuccess ||
@@ -391,7 +430,11 @@ extern "C" int mixer_server_destroy(mixer_server* sv) {
     if (sv->d2h) cudaStreamSynchronize(sv->d2h);
     if (sv->copy) cudaStreamSynchronize(sv->copy);
     for (int q = 0; q < sv->nstreams; ++q)
-        if (sv->streams[q].used) free_stream(sv->streams[q]);
+        if (sv->streams[q].used) free_stream(sv, sv->streams[q]);
+    if (sv->alloc) cudaStreamSynchronize(sv->alloc);
+    if (sv->pool) cudaMemPoolDestroy(sv->pool);
+    for (auto& kv : sv->pinned_cache) cudaFreeHost(kv.second);
+    sv->pinned_cache.clear();
     for (int t = 0; t < 2; ++t) {
         cudaFree(sv->d_maps[t]);
         cudaFree(sv->d_probs[t]);
@@ -405,6 +448,7 @@ extern "C" int mixer_server_destroy(mixer_server* sv) {
     if (sv->copy) cudaStreamDestroy(sv->copy);
     if (sv->comp) cudaStreamDestroy(sv->comp);
     if (sv->d2h) cudaStreamDestroy(sv->d2h);
+    if (sv->alloc) cudaStreamDestroy(sv->alloc);
     delete sv;
     return MIXER_OK;
 }
@@ -449,16 +493,31 @@ extern "C" int mixer_server_open(mixer_server* sv, const mixer_array_desc* d, in
     s.dump_copy_pending = false;
     cudaError_t e = cudaSuccess;
     const size_t dump_bytes = (size_t)d->nch * 2 * d->nant * d->nant * sizeof(float);
-    if ((e = cudaMalloc(&s.ring, ring_subs * s.hps * s.heap_bytes)) == cudaSuccess &&
-        (e = cudaMalloc(&s.planes, 2 * (size_t)d->nch * d->nant * s.kt)) == cudaSuccess &&
-        (e = cudaMalloc(&s.vis, (size_t)mixer_vis_elems(d->nant, d->nch) * 8)) == cudaSuccess &&
-        (e = cudaMemset(s.vis, 0, (size_t)mixer_vis_elems(d->nant, d->nch) * 8)) == cudaSuccess &&
-        (e = cudaMalloc(&s.dump_dev, dump_bytes)) == cudaSuccess &&
-        (e = cudaMalloc(&s.d_seq_err, sizeof(uint32_t))) == cudaSuccess &&
-        (e = cudaMemset(s.d_seq_err, 0, sizeof(uint32_t))) == cudaSuccess &&
+    auto palloc = [&](void** p, size_t n) {
+        return cudaMallocFromPoolAsync(p, n, sv->pool, sv->alloc);
+    };
+    const size_t vis_bytes = (size_t)mixer_vis_elems(d->nant, d->nch) * 8;
+    if ((e = palloc((void**)&s.ring, ring_subs * s.hps * s.heap_bytes)) == cudaSuccess &&
+        (e = palloc((void**)&s.planes, 2 * (size_t)d->nch * d->nant * s.kt)) == cudaSuccess &&
+        (e = palloc((void**)&s.vis, vis_bytes)) == cudaSuccess &&
+        (e = cudaMemsetAsync(s.vis, 0, vis_bytes, sv->alloc)) == cudaSuccess &&
+        (e = palloc((void**)&s.dump_dev, dump_bytes)) == cudaSuccess &&
+        (e = palloc((void**)&s.d_seq_err, sizeof(uint32_t))) == cudaSuccess &&
+        (e = cudaMemsetAsync(s.d_seq_err, 0, sizeof(uint32_t), sv->alloc)) == cudaSuccess &&
+        (e = cudaStreamSynchronize(sv->alloc)) == cudaSuccess &&   // usable on every stream
         (e = cudaEventCreateWithFlags(&s.ev_dump_copied, cudaEventDisableTiming)) == cudaSuccess &&
         (e = cudaEventCreateWithFlags(&s.ev_dump_kernel, cudaEventDisableTiming)) == cudaSuccess) {
-        for (int q = 0; q < kDumpSlots && e == cudaSuccess; ++q) e = cudaMallocHost(&s.dump[q].host, dump_bytes);
+        for (int q = 0; q < kDumpSlots && e == cudaSuccess; ++q) {
+            {
+                std::lock_guard<std::mutex> lk(sv->mu);
+                auto it = sv->pinned_cache.find(dump_bytes);
+                if (it != sv->pinned_cache.end()) {
+                    s.dump[q].host = it->second;
+                    sv->pinned_cache.erase(it);
+                }
+            }
+            if (!s.dump[q].host) e = cudaMallocHost(&s.dump[q].host, dump_bytes);
+        }
         s.ev_ready.assign(ring_subs, nullptr);
         s.ev_free.assign(ring_subs, nullptr);
         s.t_slot_done.assign(ring_subs, 0.0);
@@ -470,7 +529,7 @@ extern "C" int mixer_server_open(mixer_server* sv, const mixer_array_desc* d, in
     }
     std::lock_guard<std::mutex> lk(sv->mu);
     if (e != cudaSuccess) {
-        free_stream(s);
+        free_stream(sv, s);
         sv->bytes_used -= need;
         return mixer::cuda_status(e, "mixer_server_open");
     }
@@ -502,7 +561,7 @@ extern "C" int mixer_server_submit(mixer_server* sv, int32_t id, const void* pac
         sp = &s;
     }
     Stream& s = *sp;
-    if (sv->t_first == 0.0) sv->t_first = now_s();
+    std::vector<int64_t> completed;     // ring slots this call completed
     const uint8_t* src = static_cast<const uint8_t*>(packets);
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     int64_t done = 0;
@@ -519,11 +578,14 @@ extern "C" int mixer_server_submit(mixer_server* sv, int32_t id, const void* pac
         if ((h0 + done) % hps == 0) {   // slot complete
             MIXER_CK(cudaEventRecord(s.ev_ready[slot], sv->copy));
             s.slot_free_valid[slot] = true;
-            s.t_slot_done[slot] = now_s();
+            completed.push_back(slot);
         }
     }
     {
         std::lock_guard<std::mutex> lk(sv->mu);
+        const double t = now_s();
+        if (sv->t_first == 0.0) sv->t_first = t;
+        for (int64_t slot : completed) s.t_slot_done[slot] = t;
         s.heaps_in += nheaps;
         s.bytes_in += nheaps * s.heap_bytes;
     }
@@ -534,21 +596,33 @@ extern "C" int mixer_server_submit(mixer_server* sv, int32_t id, const void* pac
 extern "C" int mixer_server_poll(mixer_server* sv, int32_t id, mixer_dump_info* info, float* out) {
     if (!sv || !info || id < 0 || id >= (int32_t)sv->nstreams) return MIXER_EINVAL;
     collect_done(sv);
-    std::lock_guard<std::mutex> lk(sv->mu);
-    Stream& s = sv->streams[id];
-    memset(info, 0, sizeof(*info));
-    if (!s.used) return MIXER_EINVAL;
     DumpSlot* best = nullptr;
-    for (auto& d : s.dump)
-        if (d.state == 2 && (!best || d.index < best->index)) best = &d;
-    if (!best) return MIXER_OK;
-    info->available = 1;
-    info->index = best->index;
-    info->latency_s = best->t_done.load() - best->t_last_submit;
-    info->nch = s.d.nch;
-    info->nant = s.d.nant;
-    if (out) memcpy(out, best->host, (size_t)s.d.nch * 2 * s.d.nant * s.d.nant * sizeof(float));
+    size_t nbytes = 0;
+    Stream* sp;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        Stream& s = sv->streams[id];
+        memset(info, 0, sizeof(*info));
+        if (!s.used) return MIXER_EINVAL;
+        for (auto& d : s.dump)
+            if (d.state == 2 && (!best || d.index < best->index)) best = &d;
+        if (!best) return MIXER_OK;
+        info->available = 1;
+        info->index = best->index;
+        info->latency_s = best->t_done.load() - best->t_last_submit;
+        info->nch = s.d.nch;
+        info->nant = s.d.nant;
+        nbytes = (size_t)s.d.nch * 2 * s.d.nant * s.d.nant * sizeof(float);
+        best->state = 3;                 // close waits for the copy below
+        s.readers += 1;
+        sp = &s;
+    }
+    // the copy (hundreds of MB for a large array) runs without the server lock,
+    // so the worker and the submitters are not held up by it
+    if (out) memcpy(out, best->host, nbytes);
+    std::lock_guard<std::mutex> lk(sv->mu);
     best->state = 0;
+    sp->readers -= 1;
     return MIXER_OK;
 }
 
@@ -567,11 +641,18 @@ extern "C" int mixer_server_close(mixer_server* sv, int32_t id) {
     cudaStreamSynchronize(sv->comp);
     cudaStreamSynchronize(sv->d2h);
     collect_done(sv);
-    std::lock_guard<std::mutex> lk(sv->mu);
-    Stream& s = sv->streams[id];
-    sv->bytes_used -= s.bytes;
-    free_stream(s);
-    return MIXER_OK;
+    while (true) {                       // a poll may still be copying a dump out
+        {
+            std::lock_guard<std::mutex> lk(sv->mu);
+            Stream& s = sv->streams[id];
+            if (s.readers == 0) {
+                sv->bytes_used -= s.bytes;
+                free_stream(sv, s);
+                return MIXER_OK;
+            }
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(100));
+    }
 }
 
 extern "C" int mixer_server_stats(mixer_server* sv, mixer_server_counters* st) {

@@ -336,7 +336,10 @@ typedef struct mixer_server mixer_server;
  * lands in pinned host memory.  A stream's dumps equal those of
  * mixer_correlate + mixer_dump on the same packets, alone or in any mix.
  * Stream descriptors need ksub % 128 == 0.  Calls are made with the
- * server's device current. */
+ * server's device current.  Threads: different streams may be submitted to,
+ * polled and closed from different host threads; one stream's submissions
+ * come from one thread at a time.  poll and close of the same stream may run
+ * concurrently (close waits for a poll that is copying a dump out). */
 int mixer_server_create(const mixer_server_cfg* cfg, mixer_server** out);
 int mixer_server_destroy(mixer_server* sv);
 /* Device bytes one stream of `d` reserves under `cfg`. */

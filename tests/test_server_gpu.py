@@ -151,3 +151,50 @@ def test_server_backpressure(cuda):
     assert got == 2
     srv.close_stream(sid)
     srv.close()
+
+
+def test_server_poll_and_close_from_two_threads(cuda):
+    """A poller thread copying dumps out while the owner closes the stream:
+    close waits for the copy, nothing is freed under it, both calls succeed."""
+    import threading
+    import torch
+    nant, nch, tpkt, ksub, nsub, side = STREAMS["A"]
+    d = _desc(nant, nch, tpkt, ksub, 1, side)
+    hps = ksub // tpkt
+    hb = nant * (64 + 2 * nch * tpkt)
+    pk = torch.from_numpy(_packets("A", 1, seed=5)).to(cuda)
+    srv = mixer.Server(budget_bytes=8 << 30, max_streams=2, ring_subs=4, batch_subs=1)
+    sid = srv.open(d)
+    for q in range(2):                                # two dumps of one sub-integration each
+        while not srv.submit(sid, pk[q * hps * hb:], hps, seq0=1000, on_device=True):
+            time.sleep(0.01)
+    errors, polled = [], []
+    stop = threading.Event()
+
+    def poller():
+        buf = np.empty((nch, 2, nant, nant), dtype=np.float32)
+        while not stop.is_set():
+            try:
+                info = srv.poll(sid, buf)
+            except mixer.MixerError:                  # the stream is gone: expected at the end
+                break
+            except Exception as e:                    # anything else is a failure
+                errors.append(e)
+                break
+            if info is not None:
+                polled.append(info["index"])
+
+    t0 = time.time()
+    while srv.stats()["dumps"] < 1 and time.time() - t0 < 20:
+        time.sleep(0.01)
+    th = threading.Thread(target=poller)
+    th.start()
+    time.sleep(0.05)
+    srv.close_stream(sid)
+    stop.set()
+    th.join()
+    assert not errors
+    assert polled == sorted(polled) and len(set(polled)) == len(polled)
+    st = srv.stats()
+    assert st["kernel_err"] == 0 and st["bytes_used"] == 0
+    srv.close()
