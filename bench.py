@@ -8,7 +8,7 @@ Packets use the wire format (8256-byte heaps, 64-byte header, planar int8
 payload; 256 channels x 16 samples per packet).  Inputs are synthetic, made
 by the seeded packet source.
 
-One step = `--batch` sub-integrations (default 8, 4.3 GB of packets) through
+One step = `--batch` sub-integrations (default 32, 17.3 GB of packets) through
 corner-turn -> tcgen05 triangle GEMM (int32 in TMEM over the whole step) ->
 int64 integration.  `value` is device-resident throughput; `e2e` is the same
 work through the public context API from pinned host packets (host->device
@@ -51,11 +51,11 @@ PLAIN_CONFIGS = {
                   text="filled 16x16=256 elements, 128 ch, K=256, 64 sub-integrations per dump "
                        "(one step = one dump), star + planet + sigma 16 noise"),
     # the larger plain array (the headline)
-    "plain": dict(nant=1024, side=32, nch=256, ksub=1024, grid=64, sigma=8.0, noise=0, batch=8,
+    "plain": dict(nant=1024, side=32, nch=256, ksub=1024, grid=64, sigma=8.0, noise=0, batch=32,
                   text="plain array 32x32=1024 elements, 256 ch, K=1024 per sub-integration, "
                        "3 sources + sigma 8 noise, int64 integration"),
     # large-N stress: uniform int8 in [-127, 127], 128 x 128 imaging
-    "large": dict(nant=4096, side=64, nch=64, ksub=2048, grid=128, sigma=0.0, noise=1, batch=8,
+    "large": dict(nant=4096, side=64, nch=64, ksub=2048, grid=128, sigma=0.0, noise=1, batch=16,
                   text="large-N stress 64x64=4096 elements, 64 ch, K=2048 per sub-integration, "
                        "uniform int8 in [-127, 127], int64 integration, 128x128 imaging"),
 }
