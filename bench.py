@@ -633,6 +633,67 @@ def run_serve(args):
     return 0 if ok else 1
 
 
+def run_kernels(args):
+    """The path's HBM-bound kernels besides the corner-turn, on the selected plain
+    workload's cube: int32 -> int64 integration (k_vis_flush), the FP32 dump
+    (k_vis_unpack), exact int64 gridding (k_grid_tiles) and the shared-memory FFT
+    (k_image_fft).  Each launch is timed alone with CUDA events after an L2 flush
+    (a 256 MiB write), on device-resident inputs; achieved GB/s counts the
+    algorithmic bytes and is compared with the measured HBM copy bandwidth.
+    One JSON line per kernel."""
+    import torch
+    import mixer
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    N, C, side, Gs = CFG["nant"], NCH, CFG["side"], CFG["grid"]
+    nt = mixer.vis_tiles(N)
+    n = mixer.vis_elems(N, C)
+    T = N * (N + 1) // 2
+    hbm = measured_peaks().get("hbm_gbs")
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED)
+    v64 = torch.randint(-2 ** 40, 2 ** 40, (n,), dtype=torch.int64, device=dev, generator=gen)
+    v32 = torch.randint(-2 ** 30, 2 ** 30, (n,), dtype=torch.int32, device=dev, generator=gen)
+    cube = torch.empty(C * 2 * N * N, dtype=torch.float32, device=dev)
+    grid = torch.empty(C * Gs * Gs * 2, dtype=torch.int64, device=dev)
+    img = torch.empty(C * Gs * Gs, dtype=torch.float32, device=dev)
+    vmax = torch.empty(C, dtype=torch.float32, device=dev)
+    vmin = torch.empty(C, dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    cases = [
+        ("k_vis_flush", lambda: mixer.vis_flush(v32, v64, n), 24 * n,
+         "int32 read + int64 read + int64 write + int32 zeroed, per tile-packed element"),
+        ("k_vis_unpack", lambda: mixer.vis_dump_f32(v64, N, C, cube), 8 * n + 8 * C * N * N,
+         "tile-packed int64 cube read + FP32 [C][2][N][N] written"),
+        ("k_grid_tiles", lambda: mixer.grid(v64, N, C, side, Gs, grid), 16 * T * C + 16 * C * Gs * Gs,
+         "lower-triangle int64 entries read + int64 [C][G][G][2] grid written"),
+        ("k_image_fft", lambda: mixer.image_fft(grid, C, Gs, img, vmax, vmin),
+         16 * C * Gs * Gs + 4 * C * Gs * Gs,
+         "int64 grid read + FP32 image written"),
+    ]
+    for name, fn, nbytes, what in cases:
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(max(3, min(args.steps, 50))):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms = statistics.median(times)
+        gbs = nbytes / ms / 1e6
+        print(json.dumps({"kernel": name, "workload": CFG["text"], "nant": N, "nch": C,
+                          "grid": Gs, "ms": ms, "algorithmic_bytes": nbytes, "bytes": what,
+                          "gbs": gbs, "hbm_frac": gbs / hbm if hbm else None,
+                          "peak": f"of measured {hbm} GB/s" if hbm else None,
+                          "launches": len(times)}), flush=True)
+    return 0
+
+
 def run_ours(args):
     import torch
     import mixer
@@ -927,6 +988,8 @@ def main():
                     help="time the GEMM kernel over K and epilogue mode (JSON lines)")
     ap.add_argument("--profile", action="store_true",
                     help="device-resident steps only (small case for ncu captures)")
+    ap.add_argument("--kernels", action="store_true",
+                    help="time the integration, dump, gridding and FFT kernels (JSON lines)")
     args = ap.parse_args()
     configure(args.nch, args.config if args.config in PLAIN_CONFIGS else "plain")
     if args.batch <= 0:
@@ -937,6 +1000,8 @@ def main():
         return run_reference(args)
     if args.sweep_xcorr:
         return run_sweep(args)
+    if args.kernels:
+        return run_kernels(args)
     if args.config == "batched":
         return run_batched(args)
     if args.config == "serve":

@@ -45,7 +45,9 @@ __device__ __forceinline__ int pmod(int v, int g) {
     return r < 0 ? r + g : r;
 }
 
-// grid: x = tile, y = channel.  smem: window [ny][2 sx - 1][2] int64.
+// grid: x = tile, y = channel.  smem: windows re [ny][2 sx - 1] then im, int64.
+// Launched with 256 threads: a thread keeps one tile row m (one element a) and
+// walks 64 columns, four loads of each plane in flight before their adds.
 __global__ void __launch_bounds__(256)
     k_grid_tiles(const long long* __restrict__ vis, int nant, int ntiles, int sx, int G,
                  unsigned long long* __restrict__ grid) {
@@ -58,32 +60,51 @@ __global__ void __launch_bounds__(256)
     tile_window(i, j, nant, sx, dylo, ny);
     const int nx = 2 * sx - 1;
     const int ncell = ny * nx;
+    unsigned long long* win_re = win;
+    unsigned long long* win_im = win + ncell;
     for (int q = threadIdx.x; q < 2 * ncell; q += blockDim.x) win[q] = 0ull;
     if (threadIdx.x < 2) diag[threadIdx.x] = 0ull;
     __syncthreads();
 
     const long long* re = vis + (((size_t)c * ntiles + t) * 2) * 16384;
     const long long* im = re + 16384;
-    for (int e = threadIdx.x; e < 16384; e += blockDim.x) {
-        const int n = e >> 7, m = e & 127;
-        const int a = 128 * i + m, b = 128 * j + n;
-        if (a >= nant || b >= nant) continue;
-        if (i == j && m < n) continue;           // upper half of a diagonal tile
-        const long long vr = re[e], vi = im[e];
-        if (a == b) {
-            atomicAdd(&diag[0], (unsigned long long)vr);
-            atomicAdd(&diag[1], (unsigned long long)vi);
-            continue;
+    const int m = threadIdx.x & 127;             // fixed: 256 threads stride 2 columns
+    const int a = 128 * i + m;
+    const int ya = a / sx, xa = a - ya * sx;
+#pragma unroll 1
+    for (int e0 = threadIdx.x; e0 < 16384; e0 += 4 * 256) {
+        long long vr[4], vi[4];
+        int cell[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = e0 + u * 256;
+            const int n = e >> 7;
+            const int b = 128 * j + n;
+            cell[u] = -2;                        // padding, or upper half of a diagonal tile
+            vr[u] = 0;
+            vi[u] = 0;
+            if (a < nant && b < nant && !(i == j && m < n)) {
+                vr[u] = re[e];
+                vi[u] = im[e];
+                const int yb = b / sx, xb = b - yb * sx;
+                cell[u] = (a == b) ? -1 : (ya - yb - dylo) * nx + (xa - xb + sx - 1);
+            }
         }
-        const int dy = a / sx - b / sx, dx = a % sx - b % sx;
-        const int cell = (dy - dylo) * nx + (dx + sx - 1);
-        atomicAdd(&win[2 * cell + 0], (unsigned long long)vr);
-        atomicAdd(&win[2 * cell + 1], (unsigned long long)vi);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (cell[u] >= 0) {
+                atomicAdd(&win_re[cell[u]], (unsigned long long)vr[u]);
+                atomicAdd(&win_im[cell[u]], (unsigned long long)vi[u]);
+            } else if (cell[u] == -1) {
+                atomicAdd(&diag[0], (unsigned long long)vr[u]);
+                atomicAdd(&diag[1], (unsigned long long)vi[u]);
+            }
+        }
     }
     __syncthreads();
     unsigned long long* gc = grid + (size_t)c * G * G * 2;
     for (int q = threadIdx.x; q < ncell; q += blockDim.x) {
-        const unsigned long long sr = win[2 * q], si = win[2 * q + 1];
+        const unsigned long long sr = win_re[q], si = win_im[q];
         if (sr == 0ull && si == 0ull) continue;
         const int dy = q / nx + dylo, dx = q % nx - (sx - 1);
         const int f = pmod(dy, G) * G + pmod(dx, G);

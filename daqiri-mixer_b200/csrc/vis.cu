@@ -5,10 +5,10 @@
 //    stops being exact once an entry passes 2^24.
 //  * mixer_vis_dump_f32 / mixer_vis_unpack_i64: the full-square cube
 //    [C][2][N][N] of the --dump record (src/rx_host_corr.cu:187,225-227),
-//    mirrored from the lower triangle by conjugation.  One CTA per 32 x 32
-//    sub-block of a tile plane: coalesced loads along the tile's row index,
-//    a shared-memory transpose for the lower half, direct stores for the
-//    mirrored upper half.
+//    mirrored from the lower triangle by conjugation.  One CTA per 128 x 32
+//    column group of a tile plane: coalesced loads along the tile's row
+//    index, a shared-memory transpose for the lower half, direct stores for
+//    the mirrored upper half.
 #include "common.cuh"
 
 namespace mixer {
@@ -49,40 +49,56 @@ __device__ __forceinline__ long long conv<long long>(long long v) {
     return v;
 }
 
-// grid: x = 16 sub-blocks of a tile, y = tile * 2 + plane, z = channel
+// grid: x = 32-column group of a tile (4), y = tile * 2 + plane, z = channel.
+// A CTA reads 128 rows x 32 columns of one tile plane (32 KB of int64, 16
+// loads of 8 bytes a thread in flight, each warp instruction 256 contiguous
+// bytes).  The mirrored upper entries V[b][a] = conj(V[a][b]) are the tile's
+// columns, contiguous in the output too, so they are written straight from
+// registers; the lower entries V[a][b] go through a shared-memory transpose
+// (row stride 129: conflict-free both ways).
 template <typename T>
 __global__ void __launch_bounds__(256)
     k_vis_unpack(const long long* __restrict__ vis, int nant, int ntiles, T* __restrict__ out) {
-    __shared__ long long s[32][33];
-    const int sb = blockIdx.x;
-    const int mi = sb >> 2, ni = sb & 3;
+    __shared__ T s[32][129];
+    const int ng = blockIdx.x;
     const int t = blockIdx.y >> 1, p = blockIdx.y & 1;
     const int c = blockIdx.z;
     int i, j;
     decode_tile_v(t, i, j);
-    const long long* src = vis + (((size_t)c * ntiles + t) * 2 + p) * 16384;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int r = ty; r < 32; r += 8) {
-        const int n = 32 * ni + r, m = 32 * mi + tx;
-        s[r][tx] = src[n * 128 + m];
-    }
-    __syncthreads();
+    const long long* src =
+        vis + (((size_t)c * ntiles + t) * 2 + p) * 16384 + (size_t)(32 * ng) * 128;
     T* plane = out + ((size_t)c * 2 + p) * (size_t)nant * nant;
-    // V[a][b], a = 128 i + m (row), b = 128 j + n (column): b contiguous
-    for (int r = ty; r < 32; r += 8) {
-        const int m = 32 * mi + r, n = 32 * ni + tx;
-        const int a = 128 * i + m, b = 128 * j + n;
-        if (a < nant && b < nant) plane[(size_t)a * nant + b] = conv<T>(s[tx][r]);
-    }
-    if (i != j) {   // mirrored entry V[b][a] = conj(V[a][b]): a contiguous
-        for (int r = ty; r < 32; r += 8) {
-            const int n = 32 * ni + r, m = 32 * mi + tx;
-            const int a = 128 * i + m, b = 128 * j + n;
-            if (a < nant && b < nant) {
-                const long long v = s[r][tx];
-                plane[(size_t)b * nant + a] = p ? conv<T>(-v) : conv<T>(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int a0 = 128 * i, b0 = 128 * j + 32 * ng;
+    long long v[4][4];   // column w + 8 q, row lane + 32 r
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) v[q][r] = src[(w + 8 * q) * 128 + lane + 32 * r];
+    if (i != j) {        // mirrored entry V[b][a]: a contiguous
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int b = b0 + w + 8 * q;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int a = a0 + lane + 32 * r;
+                if (a < nant && b < nant)
+                    plane[(size_t)b * nant + a] = p ? conv<T>(-v[q][r]) : conv<T>(v[q][r]);
             }
         }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) s[w + 8 * q][lane + 32 * r] = conv<T>(v[q][r]);
+    __syncthreads();
+    // V[a][b], a = 128 i + m (row), b = 128 j + 32 ng + lane: b contiguous
+    const int b = b0 + lane;
+#pragma unroll 4
+    for (int k = 0; k < 16; ++k) {
+        const int m = 16 * w + k;
+        const int a = a0 + m;
+        if (a < nant && b < nant) plane[(size_t)a * nant + b] = s[lane][m];
     }
 }
 
@@ -91,7 +107,7 @@ int unpack(const int64_t* vis64, int32_t nant, int32_t nch, T* out, void* stream
     if (!vis64 || !out || nant <= 0 || nch <= 0 || nch > 65535) return MIXER_EINVAL;
     const int nt = mixer_vis_tiles(nant);
     if (2 * nt > 65535) return MIXER_EINVAL;
-    dim3 grid(16, (unsigned)(2 * nt), (unsigned)nch);
+    dim3 grid(4, (unsigned)(2 * nt), (unsigned)nch);
     k_vis_unpack<T><<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
         reinterpret_cast<const long long*>(vis64), nant, nt, out);
     MIXER_CK(cudaGetLastError());

@@ -165,6 +165,30 @@ def test_xcorr_cta_cap_is_exact(cuda, max_ctas):
     assert np.array_equal(v64.cpu().numpy(), ref)
 
 
+def test_xcorr_partial_last_round_is_exact(cuda):
+    """256 elements x 128 channels = 384 tile items on 148 persistent CTAs: the
+    last round is partly empty and two thirds of the tiles are diagonal.  The
+    int64 accumulate and int32 store launches give the same cube, equal to the
+    oracle's exact sums on the first channels."""
+    import torch
+    rng = np.random.default_rng(41)
+    nant, nch, kt = 256, 128, 16384
+    planes = _rand_planes(rng, nch, nant, kt)
+    dpl = _t(planes, cuda)
+    n = mixer.vis_elems(nant, nch)
+    v32 = _zeros(n, torch.int32, cuda)
+    v64 = _zeros(n, torch.int64, cuda)
+    err = _zeros(1, torch.int32, cuda)
+    mixer.xcorr_tri(dpl, nant, nch, kt, 0, kt, mixer.VIS_STORE_I32, v32, err)
+    mixer.xcorr_tri(dpl, nant, nch, kt, 0, kt, mixer.VIS_ACC_I64, v64, err)
+    _sync()
+    assert int(err.item()) == 0
+    assert np.array_equal(v64.cpu().numpy(), v32.cpu().numpy().astype(np.int64))
+    sub = 4                                                # oracle on the first channels
+    ref = oracle.vis_tile_pack(oracle.correlate(planes, nc=sub)).reshape(-1)
+    assert np.array_equal(v64[:ref.size].cpu().numpy(), ref)
+
+
 def test_xcorr_extreme_inputs(cuda):
     """-128 everywhere: exact here; the reference's -A_im (src/cgemm.cuh:52) wraps."""
     import torch
