@@ -30,6 +30,7 @@
 //               (warp - 2) / 4)
 #include "common.cuh"
 #include "xcorr.cuh"
+#include <cstdlib>
 #include <cstring>
 
 namespace mixer {
@@ -352,6 +353,285 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+// =============================================================================
+// Pair kernel: one work item per cluster of two CTAs on two SMs.
+//
+// tcgen05 cta_group::2.  The pair's leader (cluster rank 0) issues M 256 x
+// N 256 MMAs: A's 256 rows are 128 from each CTA's shared memory, and the
+// 256-row B operand [Xr_j ; Xi_j] is split with Xr_j in the leader and Xi_j
+// in the peer (same offsets).  Each CTA's TMEM then holds the four products
+// of its own 128-row block against column block j,
+//   D1 = Xr_a [Xr_j ; Xi_j]^T = [R1 | P2],  D2 = Xi_a [Xr_j ; Xi_j]^T = [P1 | R2],
+// so one item computes two tiles (a0, j), (a1, j) that share column block j.
+// Per SM and 32-sample step the tensor cores read 16 KB of shared memory
+// instead of 24 KB and TMA writes 12 KB instead of 16 KB: 112 instead of 160
+// bytes per clock at the full MMA rate.  Stages are 48 KB, four of them.
+//
+// Pairing.  Column block j holds tiles (i, j), i = j .. nb-1.  Consecutive
+// rows pair up; a column with an odd count leaves its last tile (nb-1, j).
+// Those leftovers share ROW block nb-1, so they pair as the products
+// X_j X_{nb-1}^H against B = block nb-1, and the epilogue writes tile element
+// (m, n) = conj(D[n][m]) (for the diagonal tile this is D itself).  Per
+// channel: f(nb) = floor(nb^2/4) regular pairs, column j's first at
+// f(nb) - f(nb - j), then ceil(ceil(nb/2)/2) leftover pairs; when ceil(nb/2)
+// is odd the last leftover pair has no second tile and its peer half is
+// computed and discarded.
+// =============================================================================
+constexpr int kPairStages = 4;
+constexpr int kPairStageBytes = 3 * kTileBytes;   // A_re, A_im, this CTA's half of B
+constexpr int kPairSmemBytes = kPairStages * kPairStageBytes + 1024 + kBarBytes;
+constexpr uint32_t kIdescPair = idesc_i8(256, 256);
+static_assert(kPairSmemBytes <= 232448, "shared memory");
+
+struct PairArgs {
+    int32_t nant, nch, nblk, ntiles;
+    int32_t kbeg, nkc;   // first sample, number of 128-sample chunks
+    int32_t mode;
+    int32_t nreg;        // regular pairs per channel
+    int32_t npairs;      // pairs per channel
+    int32_t pad_;
+    int64_t nwork;       // nch * npairs
+    void* vis;
+    int32_t* err;
+};
+
+// This CTA's half of pair item w.
+struct PairHalf {
+    int c, a, j, t;      // channel, A row block, B column block, stored tile
+    bool valid, transposed;
+};
+
+__device__ __forceinline__ int quarter_sq(int n) { return (n * n) >> 2; }
+
+__device__ __forceinline__ PairHalf pair_half(const PairArgs& g, int64_t w, int rank) {
+    PairHalf h;
+    h.c = (int)(w / g.npairs);
+    const int p = (int)(w - (int64_t)h.c * g.npairs);
+    const int nb = g.nblk;
+    if (p < g.nreg) {
+        // column j = nb - n with n the smallest count whose f(n) >= q
+        const int q = g.nreg - p;
+        int n = (int)(2.0f * sqrtf((float)q));
+        if (n < 2) n = 2;
+        while (quarter_sq(n) < q) ++n;
+        while (n > 2 && quarter_sq(n - 1) >= q) --n;
+        h.j = nb - n;
+        h.a = h.j + 2 * (quarter_sq(n) - q) + rank;
+        h.t = h.a * (h.a + 1) / 2 + h.j;
+        h.valid = true;
+        h.transposed = false;
+    } else {
+        const int s = 2 * (p - g.nreg) + rank;          // leftover of column nb-1-2s
+        h.j = nb - 1;
+        h.valid = s < ((nb + 1) >> 1);
+        h.a = h.valid ? nb - 1 - 2 * s : nb - 1;
+        h.t = (nb - 1) * nb / 2 + h.a;                  // tile (nb-1, a)
+        h.transposed = true;
+    }
+    return h;
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_xcorr_pair(const __grid_constant__ CUtensorMap tmap, const PairArgs args) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;            // same offset in both CTAs
+    uint8_t* gbase = smem_raw + (base - raw);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + kPairStages * kPairStageBytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kPairStages + 4);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const bool leader = (rank == 0);
+    const int64_t cid = blockIdx.x >> 1, ncl = gridDim.x >> 1;
+    const int FULL = 0, EMPTY = kPairStages, ACCF = 2 * kPairStages, ACCE = 2 * kPairStages + 1,
+              DRAIN = 2 * kPairStages + 2;
+    auto bar = [&](int k) { return smem_u32(&bars[k]); };
+    // A wait that gives up stops both CTAs of the pair.
+    auto raise_abort = [&]() {
+        *abort_flag = 1;
+        st_cluster_u32(mapa_shared(smem_u32((const void*)abort_flag), rank ^ 1u), 1u);
+    };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kPairStages; ++s) {
+            mbar_init(bar(FULL + s), 1);      // leader: its expect_tx + both CTAs' bytes
+            mbar_init(bar(EMPTY + s), 1);     // the leader's multicast commit
+        }
+        mbar_init(bar(ACCF), 1);
+        mbar_init(bar(ACCE), 2 * 32 * kEpiWarps);   // leader: every epilogue thread of both
+        mbar_init(bar(DRAIN), 1);
+        *abort_flag = 0;
+        fence_mbar_init();
+    }
+    if (warp == 0 && lane == 0) prefetch_tmap(&tmap);
+    if (warp == 1) {
+        tmem_alloc_pair(smem_u32(tmem_slot), kTmemCols);
+        tmem_relinquish_pair();
+    }
+    tc_fence_before();
+    cluster_sync_all();                       // barriers and TMEM ready in both CTAs
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer (both)
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            bool ok = true;
+            for (int64_t w = cid; w < args.nwork && ok; w += ncl) {
+                const PairHalf h = pair_half(args, w, (int)rank);
+                for (int kc = 0; kc < args.nkc; ++kc) {
+                    if (!mbar_wait(bar(EMPTY + stage), phase ^ 1u, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t sb = base + stage * kPairStageBytes;
+                    const uint32_t fb = mapa_shared(bar(FULL + stage), 0);
+                    if (leader) mbar_expect_tx(bar(FULL + stage), 2 * kPairStageBytes);
+                    const int k = args.kbeg + kc * kKc;
+                    tma_load_4d_pair(sb, &tmap, fb, k, h.a * kTile, h.c, 0);
+                    tma_load_4d_pair(sb + kTileBytes, &tmap, fb, k, h.a * kTile, h.c, 1);
+                    tma_load_4d_pair(sb + 2 * kTileBytes, &tmap, fb, k, h.j * kTile, h.c, (int)rank);
+                    if (++stage == kPairStages) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+            }
+            if (!ok) {
+                if (args.err) atomicOr(args.err, 1);
+                raise_abort();
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer (leader)
+        if (lane == 0 && leader) {
+            int stage = 0;
+            uint32_t phase = 0, acc_phase = 0;
+            bool ok = true;
+            int64_t consumed = 0;
+            const uint32_t t_d1 = tmem, t_d2 = tmem + 256;
+            for (int64_t w = cid; w < args.nwork; w += ncl) {
+                if (!mbar_wait(bar(ACCE), acc_phase ^ 1u, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                for (int kc = 0; kc < args.nkc; ++kc) {
+                    if (!mbar_wait(bar(FULL + stage), phase, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sb = base + stage * kPairStageBytes;
+                    const uint64_t ar = sdesc(sb);
+                    const uint64_t ai = sdesc(sb + kTileBytes);
+                    const uint64_t b = sdesc(sb + 2 * kTileBytes);
+#pragma unroll
+                    for (int kk = 0; kk < kKc / 32; ++kk) {
+                        const uint64_t o = (uint64_t)((kk * 32) >> 4);   // 32-byte K step
+                        const uint32_t acc = (kc > 0 || kk > 0) ? 1u : 0u;
+                        mma_i8_pair(t_d1, ar + o, b + o, kIdescPair, acc);
+                        mma_i8_pair(t_d2, ai + o, b + o, kIdescPair, acc);
+                    }
+                    tc_commit_pair(bar(EMPTY + stage), 0x3);   // stage free in both CTAs
+                    ++consumed;
+                    if (++stage == kPairStages) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                tc_commit_pair(bar(ACCF), 0x3);               // both CTAs' accumulators
+                acc_phase ^= 1u;
+            }
+            if (!ok) {
+                if (args.err) atomicOr(args.err, 2);
+                raise_abort();
+                // Let loads already counted on this CTA's barriers land.
+                for (int64_t q = consumed; q < consumed + kPairStages; ++q)
+                    mbar_wait(bar(FULL + (int)(q % kPairStages)), (uint32_t)((q / kPairStages) & 1));
+            }
+            // No MMA may still be writing either CTA's TMEM when it is released:
+            // the peer deallocates only after the closing cluster barrier,
+            // which this thread reaches after the wait.
+            tc_commit_pair(bar(DRAIN), 0x1);
+            mbar_wait(bar(DRAIN), 0);
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue (both)
+        const int q = warp & 3;
+        const int col0 = kEpiCols * ((warp - 2) >> 2);
+        const int m = q * 32 + lane;
+        const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col0;
+        const uint32_t acce = mapa_shared(bar(ACCE), 0);
+        uint32_t acc_phase = 0;
+        for (int64_t w = cid; w < args.nwork; w += ncl) {
+            const PairHalf h = pair_half(args, w, (int)rank);
+            if (!mbar_wait(bar(ACCF), acc_phase, abort_flag)) {
+                if (args.err) atomicOr(args.err, 4);
+                raise_abort();
+                break;
+            }
+            tc_fence_after();
+            const size_t tb = ((size_t)h.c * args.ntiles + h.t) * (size_t)(2 * kTile * kTile);
+#pragma unroll 1
+            for (int n0 = 0; n0 < kEpiCols; n0 += 16) {
+                uint32_t r[4][16];   // R1, P2, P1, R2
+                tmem_ld4_x16(trow + n0, trow + 128 + n0, trow + 256 + n0, trow + 384 + n0, r);
+                if (n0 == kEpiCols - 16) {           // this warp's TMEM reads are done
+                    tc_fence_before();
+                    mbar_arrive_cluster(acce);
+                }
+                if (!h.valid) continue;
+                // plain tile: element (m, n) at n * 128 + m; conjugate transpose:
+                // D[m][n] goes to element (n, m), at m * 128 + n, with Im negated
+                const size_t e0 = h.transposed ? tb + (size_t)m * kTile + (col0 + n0)
+                                               : tb + (size_t)(col0 + n0) * kTile + m;
+                const int es = h.transposed ? 1 : kTile;
+                const int sg = h.transposed ? -1 : 1;
+                if (args.mode == MIXER_VIS_ACC_I64) {
+                    unsigned long long* v = reinterpret_cast<unsigned long long*>(args.vis) + e0;
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        atomicAdd(v + e * es, (unsigned long long)(long long)(int32_t)(r[0][e] + r[3][e]));
+                        atomicAdd(v + e * es + kTile * kTile,
+                                  (unsigned long long)(long long)(sg * (int32_t)(r[2][e] - r[1][e])));
+                    }
+                } else if (args.mode == MIXER_VIS_ACC_I32) {
+                    int* v = reinterpret_cast<int*>(args.vis) + e0;
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        atomicAdd(v + e * es, (int)(r[0][e] + r[3][e]));
+                        atomicAdd(v + e * es + kTile * kTile, sg * (int)(r[2][e] - r[1][e]));
+                    }
+                } else {
+                    int* v = reinterpret_cast<int*>(args.vis) + e0;
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        v[e * es] = (int)(r[0][e] + r[3][e]);
+                        v[e * es + kTile * kTile] = sg * (int)(r[2][e] - r[1][e]);
+                    }
+                }
+            }
+            acc_phase ^= 1u;
+        }
+    }
+
+    // Neither CTA leaves while the pair may still use its shared memory or TMEM.
+    tc_fence_before();
+    cluster_sync_all();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc_pair(tmem, kTmemCols);
+    }
+}
+
+
 using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                               const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
                               const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -410,6 +690,84 @@ static int set_smem_attr() {
 
 int xcorr_sm_count() { return sm_count(); }
 
+// Pair kernel set-up, once per device: its shared-memory attribute and how
+// many clusters of two CTAs can be resident at once (0: pairs unusable).
+static int pair_clusters() {
+    static int clusters[64];
+    static uint64_t done = 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64) return 0;
+    if (!(done & (1ull << dev))) {
+        int n = 0;
+        if (cudaFuncSetAttribute(k_xcorr_pair, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kPairSmemBytes) == cudaSuccess) {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = 2;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(2 * 74);
+            cfg.blockDim = dim3(kThreads);
+            cfg.dynamicSmemBytes = kPairSmemBytes;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            if (cudaOccupancyMaxActiveClusters(&n, k_xcorr_pair, &cfg) != cudaSuccess) n = 0;
+        }
+        cudaGetLastError();   // a refused query leaves no error behind
+        clusters[dev] = n;
+        done |= 1ull << dev;
+    }
+    return clusters[dev];
+}
+
+// The pair kernel is opt-in (MIXER_XCORR_PAIRS=1 in the environment), from
+// three 128-row blocks up (at most one discarded half per channel).  Measured
+// on one B200 it is no faster than the one-SM kernel at boost clock and
+// slower under the power cap (the clock settles lower: each SM still needs
+// all of B, half of it from the peer), so the one-SM kernel is the default.
+static bool pairs_wanted(int nblk) {
+    if (kKc != 128 || nblk < 3) return false;
+    const char* e = getenv("MIXER_XCORR_PAIRS");
+    return e && e[0] == '1';
+}
+
+static int pair_launch(const CUtensorMap& map, int32_t nant, int32_t nch, int64_t kbeg,
+                       int64_t klen, int32_t mode, void* vis, int32_t max_ctas, int32_t* err,
+                       int clusters, cudaStream_t st) {
+    PairArgs a;
+    memset(&a, 0, sizeof(a));
+    a.nant = nant;
+    a.nch = nch;
+    a.nblk = (nant + kTile - 1) / kTile;
+    a.ntiles = a.nblk * (a.nblk + 1) / 2;
+    a.kbeg = (int32_t)kbeg;
+    a.nkc = (int32_t)((klen + kKc - 1) / kKc);
+    a.mode = mode;
+    a.nreg = a.nblk * a.nblk / 4;
+    a.npairs = a.nreg + ((a.nblk + 1) / 2 + 1) / 2;
+    a.nwork = (int64_t)nch * a.npairs;
+    a.vis = vis;
+    a.err = err;
+    int64_t ncl = clusters;
+    if (max_ctas > 0 && max_ctas / 2 < ncl) ncl = max_ctas / 2;
+    if (a.nwork < ncl) ncl = a.nwork;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3((unsigned)(2 * ncl));
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = kPairSmemBytes;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    MIXER_CK(cudaLaunchKernelEx(&cfg, k_xcorr_pair, map, a));
+    return MIXER_OK;
+}
+
 // Launch over samples [kbeg, kbeg + klen) with klen <= MIXER_KMAX_I32.
 // At most max_ctas persistent CTAs (<= 0: one per SM).
 static int xcorr_launch(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt, int64_t kbeg,
@@ -418,6 +776,11 @@ static int xcorr_launch(const int8_t* planes, int32_t nant, int32_t nch, int64_t
     CUtensorMap map;
     int rc = xcorr_encode_map(&map, planes, nant, nch, kt, kbeg + klen);
     if (rc != MIXER_OK) return rc;
+    if (max_ctas != 1 && pairs_wanted((nant + kTile - 1) / kTile)) {
+        const int clusters = pair_clusters();
+        if (clusters > 0)
+            return pair_launch(map, nant, nch, kbeg, klen, mode, vis, max_ctas, err, clusters, st);
+    }
     rc = set_smem_attr();
     if (rc != MIXER_OK) return rc;
     XcorrArgs a;

@@ -100,14 +100,20 @@ int mixer_corner_turn(const uint8_t* packets, int64_t pkt_stride, int32_t hdr_by
  * int32 for the *_I32 modes, int64 for MIXER_VIS_ACC_I64.  For the I32 modes
  * klen <= MIXER_KMAX_I32; the I64 mode splits longer ranges itself.
  * err: device int32 (may be NULL) that receives MIXER_ETIMEOUT bits if a
- * bounded wait in the kernel ever gave up.  kt % 16 == 0. */
+ * bounded wait in the kernel ever gave up.  kt % 16 == 0.
+ * With MIXER_XCORR_PAIRS=1 in the environment and nant > 256 (three 128-row
+ * blocks) the work runs on pairs of SMs instead (clusters of two CTAs, tcgen05
+ * cta_group::2); both kernels give the same cube.  The one-SM kernel is the
+ * default: on B200 the pair kernel measured no faster at boost clock and
+ * slower under the power cap. */
 int mixer_xcorr_tri(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt,
                     int64_t kbeg, int64_t klen, int32_t mode, void* vis,
                     int32_t* err, void* stream);
 
-/* Same, with at most max_ctas persistent CTAs (<= 0: one per SM).  Leaving
- * SMs free lets an HBM-bound kernel on another stream (the next corner-turn)
- * run beside the tensor-bound GEMM. */
+/* Same, with at most max_ctas persistent CTAs (<= 0: one per SM; the pair
+ * kernel uses max_ctas / 2 clusters, and max_ctas == 1 selects the one-SM
+ * kernel).  Leaving SMs free lets an HBM-bound kernel on another stream (the
+ * next corner-turn) run beside the tensor-bound GEMM. */
 int mixer_xcorr_tri_ex(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt,
                        int64_t kbeg, int64_t klen, int32_t mode, void* vis,
                        int32_t max_ctas, int32_t* err, void* stream);

@@ -148,10 +148,13 @@ def test_xcorr_accumulate_modes(cuda):
     assert int(v32.abs().max().item()) == 0
 
 
+@pytest.mark.parametrize("pairs", ["0", "1"])
 @pytest.mark.parametrize("max_ctas", [1, 7, 100000])
-def test_xcorr_cta_cap_is_exact(cuda, max_ctas):
-    """mixer_xcorr_tri_ex: fewer persistent CTAs walk more items each, same cube."""
+def test_xcorr_cta_cap_is_exact(cuda, monkeypatch, max_ctas, pairs):
+    """mixer_xcorr_tri_ex: fewer persistent CTAs walk more items each, same cube
+    (one-SM kernel, and the pair kernel with max_ctas / 2 clusters)."""
     import torch
+    monkeypatch.setenv("MIXER_XCORR_PAIRS", pairs)
     rng = np.random.default_rng(31 + max_ctas)
     nant, nch, kt = 384, 3, 512
     planes = _rand_planes(rng, nch, nant, kt)
@@ -163,6 +166,57 @@ def test_xcorr_cta_cap_is_exact(cuda, max_ctas):
     assert int(err.item()) == 0
     ref = oracle.vis_tile_pack(oracle.correlate(planes)).reshape(-1)
     assert np.array_equal(v64.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("nant,nch,kt,kbeg,klen,mode", [
+    (384, 3, 512, 0, 512, "store"),      # 3 row blocks: 3 pairs, one leftover pair
+    (512, 2, 256, 0, 256, "acc64"),      # 4 blocks: 5 pairs
+    (640, 2, 384, 128, 256, "store"),    # 5 blocks: last leftover pair has one tile
+    (1000, 2, 208, 16, 176, "acc64"),    # 8 blocks, ragged N and K
+    (1024, 4, 1024, 0, 1024, "acc32"),   # 8 blocks, 18 pairs per channel
+])
+def test_xcorr_pairs_match_oracle(cuda, monkeypatch, nant, nch, kt, kbeg, klen, mode):
+    """MIXER_XCORR_PAIRS=1: from three 128-row blocks up the GEMM runs on pairs
+    of SMs (tcgen05 cta_group::2): two tiles that share a column block per
+    cluster, leftover tiles as conjugate-transposed products.  Every mode is
+    exact."""
+    import torch
+    monkeypatch.setenv("MIXER_XCORR_PAIRS", "1")
+    rng = np.random.default_rng(nant + kt + klen)
+    planes = _rand_planes(rng, nch, nant, kt)
+    dt = torch.int64 if mode == "acc64" else torch.int32
+    vis = _zeros(mixer.vis_elems(nant, nch), dt, cuda)
+    err = _zeros(1, torch.int32, cuda)
+    md = {"store": mixer.VIS_STORE_I32, "acc32": mixer.VIS_ACC_I32, "acc64": mixer.VIS_ACC_I64}[mode]
+    mixer.xcorr_tri(_t(planes, cuda), nant, nch, kt, kbeg, klen, md, vis, err)
+    _sync()
+    assert int(err.item()) == 0
+    ref = oracle.vis_tile_pack(oracle.correlate(planes, kbeg=kbeg, klen=klen)).reshape(-1)
+    assert np.array_equal(vis.cpu().numpy().astype(np.int64), ref)
+
+
+def test_xcorr_pairs_equal_single_sm(cuda, monkeypatch):
+    """The pair kernel (MIXER_XCORR_PAIRS=1) and the one-SM kernel give the same
+    cube, including -128 inputs and the int32 bound of one launch."""
+    import torch
+    rng = np.random.default_rng(77)
+    nant, nch, kt = 768, 2, 65408
+    planes = rng.integers(-128, 128, size=(2, nch, nant, kt), dtype=np.int8)
+    planes[:, :, :128] = -128                        # one row block at the extreme
+    dpl = _t(planes, cuda)
+    n = mixer.vis_elems(nant, nch)
+    out = []
+    for env in ("1", "0"):
+        monkeypatch.setenv("MIXER_XCORR_PAIRS", env)
+        v = _zeros(n, torch.int32, cuda)
+        err = _zeros(1, torch.int32, cuda)
+        mixer.xcorr_tri(dpl, nant, nch, kt, 0, kt, mixer.VIS_STORE_I32, v, err)
+        _sync()
+        assert int(err.item()) == 0
+        out.append(v.cpu().numpy())
+    assert np.array_equal(out[0], out[1])
+    ref = oracle.vis_tile_pack(oracle.correlate(planes, nc=1)).reshape(-1)
+    assert np.array_equal(out[0][:ref.size].astype(np.int64), ref)
 
 
 def test_xcorr_partial_last_round_is_exact(cuda):
