@@ -47,7 +47,8 @@ __device__ __forceinline__ int pmod(int v, int g) {
 
 // grid: x = tile, y = channel.  smem: windows re [ny][2 sx - 1] then im, int64.
 // Launched with 256 threads: a thread keeps one tile row m (one element a) and
-// walks 64 columns, four loads of each plane in flight before their adds.
+// walks every other column, four loads of each plane in flight before their
+// adds, with the column element's array position advanced instead of divided.
 __global__ void __launch_bounds__(256)
     k_grid_tiles(const long long* __restrict__ vis, int nant, int ntiles, int sx, int G,
                  unsigned long long* __restrict__ grid) {
@@ -68,26 +69,38 @@ __global__ void __launch_bounds__(256)
 
     const long long* re = vis + (((size_t)c * ntiles + t) * 2) * 16384;
     const long long* im = re + 16384;
-    const int m = threadIdx.x & 127;             // fixed: 256 threads stride 2 columns
+    const int m = threadIdx.x & 127;             // this thread's tile row
     const int a = 128 * i + m;
     const int ya = a / sx, xa = a - ya * sx;
+    // Columns n = n0, n0 + 2, ... below nlim: the array's last element and, on a
+    // diagonal tile, the row itself (the upper half is the mirror image).
+    int nlim = nant - 128 * j;
+    if (nlim > 128) nlim = 128;
+    if (i == j && nlim > m + 1) nlim = m + 1;
+    if (a >= nant) nlim = 0;
+    int n = threadIdx.x >> 7;
+    int yb = (128 * j + n) / sx;                 // the column element's array position,
+    int xb = 128 * j + n - yb * sx;              // advanced by two columns a step
+    const int cbase = (ya - dylo) * nx + xa + sx - 1;   // cell = cbase - yb * nx - xb
 #pragma unroll 1
-    for (int e0 = threadIdx.x; e0 < 16384; e0 += 4 * 256) {
+    for (; n < nlim; n += 8) {
         long long vr[4], vi[4];
         int cell[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const int e = e0 + u * 256;
-            const int n = e >> 7;
-            const int b = 128 * j + n;
-            cell[u] = -2;                        // padding, or upper half of a diagonal tile
+            const int nn = n + 2 * u;
+            cell[u] = -2;
             vr[u] = 0;
             vi[u] = 0;
-            if (a < nant && b < nant && !(i == j && m < n)) {
-                vr[u] = re[e];
-                vi[u] = im[e];
-                const int yb = b / sx, xb = b - yb * sx;
-                cell[u] = (a == b) ? -1 : (ya - yb - dylo) * nx + (xa - xb + sx - 1);
+            if (nn < nlim) {
+                vr[u] = re[nn * 128 + m];
+                vi[u] = im[nn * 128 + m];
+                cell[u] = (a == 128 * j + nn) ? -1 : cbase - yb * nx - xb;
+            }
+            xb += 2;
+            while (xb >= sx) {
+                xb -= sx;
+                ++yb;
             }
         }
 #pragma unroll
