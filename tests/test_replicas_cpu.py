@@ -37,7 +37,7 @@ def test_two_replicas_reduce_over_gloo():
     if torch.cuda.is_available():
         return   # on a GPU box bench.py selects NCCL; this checks the CPU / gloo path
     world = 2
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()   # no fork of this multi-threaded process
     out = mgr.dict()
     mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
     assert out[0] == (0, 2, 11.0, 300.0)
