@@ -694,6 +694,45 @@ def run_kernels(args):
     return 0
 
 
+def mma_probe(torch, mixer, dev, local=0, runs=(("burst", 20000, 5), ("sustained", 200000, 20))):
+    """Dense int8 tensor-core rate of this GPU with the GEMM's own MMA stream
+    (mixer_mma_peak: resident shared-memory operands, no loads), with the SM
+    clock sampled: the measured int8 ceiling beside the 2 x bf16 figure."""
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mixer.mma_peak(1000, 0, err)
+    torch.cuda.synchronize()
+    out = []
+    for label, iters, reps in runs:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            e0.record()
+            for _ in range(reps):
+                mixer.mma_peak(iters, 0, err)
+            e1.record()
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        ops = float(sms) * iters * reps * mixer.MMA_PEAK_OPS_PER_ITER
+        c = clk.summary()
+        tops = ops / ms / 1e9
+        out.append({"probe": "int8 MMA peak (tcgen05 kind::i8, M128 N256 K32, smem operands)",
+                    "run": label, "ms": ms, "tops": tops, "clocks": c,
+                    "ops_per_sm_per_clock": (tops * 1e12 / (sms * c["sm_mhz"] * 1e6)
+                                             if c.get("sm_mhz") else None),
+                    "kernel_err": int(err.item())})
+    return out
+
+
+def run_mma_peak(args):
+    import torch
+    import mixer
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    for line in mma_probe(torch, mixer, dev):
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args):
     import torch
     import mixer
@@ -868,6 +907,25 @@ def run_ours(args):
         "gpu_launches": 2 * args.steps,
         "e2e": e2e,
     }
+    # ---- the GEMM against the measured int8 tensor-core rate --------------------
+    # The probe runs the GEMM's MMA stream with no memory traffic: per clock it is
+    # the rate the tensor cores can reach; under the power cap it also holds a
+    # higher clock than the GEMM, whose operand and cube traffic draw power too.
+    probe = {r["run"]: r for r in mma_probe(torch, mixer, dev, local)}
+    gemm_tile_tops = achieved * (mixer.vis_tiles(NANT) * 128 * 128) / (NANT * (NANT + 1) / 2)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    gmhz = line["clocks"].get("sm_mhz")
+    sus = probe["sustained"]
+    line["int8_mma_probe"] = {
+        "burst_tops": probe["burst"]["tops"], "burst_mhz": probe["burst"]["clocks"].get("sm_mhz"),
+        "sustained_tops": sus["tops"], "sustained_mhz": sus["clocks"].get("sm_mhz"),
+        "probe_ops_per_sm_per_clock": sus["ops_per_sm_per_clock"],
+        "gemm_tile_basis_tops": gemm_tile_tops,
+        "gemm_ops_per_sm_per_clock": gemm_tile_tops * 1e12 / (sms * gmhz * 1e6) if gmhz else None,
+        "gemm_per_clock_frac": (gemm_tile_tops * 1e12 / (sms * gmhz * 1e6) / sus["ops_per_sm_per_clock"]
+                                if gmhz and sus["ops_per_sm_per_clock"] else None),
+        "gemm_frac_of_sustained_probe": gemm_tile_tops / sus["tops"],
+        "what": "tile basis (every computed 128 x 128 tile); the probe is mixer_mma_peak"}
     # ---- imaging of the integrated cube (grid + FFT), device resident ------------
     with mixer.ArrayContext(nant=NANT, nch=NCH, tpkt=TPKT, ksub=KSUB, nsub_dump=1, side_x=SIDE,
                             grid=G, pkt_stride=STRIDE, hdr_bytes=HDR, max_heaps=HEAPS_PER_SUB) as ic:
@@ -993,6 +1051,8 @@ def main():
                     help="time the GEMM kernel over K and epilogue mode (JSON lines)")
     ap.add_argument("--profile", action="store_true",
                     help="device-resident steps only (small case for ncu captures)")
+    ap.add_argument("--mma-peak", action="store_true",
+                    help="measure the dense int8 tensor-core rate (burst and sustained)")
     ap.add_argument("--kernels", action="store_true",
                     help="time the integration, dump, gridding and FFT kernels (JSON lines)")
     args = ap.parse_args()
@@ -1007,6 +1067,8 @@ def main():
         return run_sweep(args)
     if args.kernels:
         return run_kernels(args)
+    if args.mma_peak:
+        return run_mma_peak(args)
     if args.config == "batched":
         return run_batched(args)
     if args.config == "serve":

@@ -632,6 +632,57 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 
+// Dense int8 tensor-core rate with the GEMM's own instruction stream: one CTA
+// per SM issues `iters` times the k_xcorr_tri K-step (two M 128 x N 256 x K 32
+// kind::i8 MMAs per 32 samples, four steps per 128-byte stage) from one
+// resident shared-memory stage, with no loads, into the same 512 TMEM columns.
+// The operand bytes are pseudo-random so the tensor cores draw realistic power.
+__global__ void __launch_bounds__(128, 1) k_mma_peak(int64_t iters, int32_t* err) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    uint8_t* gbase = smem_raw + (base - raw);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(gbase + kStageBytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+    const int warp = threadIdx.x >> 5;
+    for (int q = threadIdx.x; q < kStageBytes / 4; q += blockDim.x)
+        reinterpret_cast<uint32_t*>(gbase)[q] = (uint32_t)q * 2654435761u ^ 0x9e3779b9u;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (threadIdx.x == 0) {
+        mbar_init(smem_u32(bar), 1);
+        fence_mbar_init();
+    }
+    if (warp == 1) {
+        tmem_alloc(smem_u32(tmem_slot), kTmemCols);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    if (threadIdx.x == 0) {
+        const uint64_t ar = sdesc(base), ai = sdesc(base + kTileBytes), b = sdesc(base + 2 * kTileBytes);
+        for (int64_t it = 0; it < iters; ++it) {
+#pragma unroll
+            for (int kk = 0; kk < kKc / 32; ++kk) {
+                const uint64_t o = (uint64_t)((kk * 32) >> 4);
+                const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
+                mma_i8(tmem, ar + o, b + o, kIdesc, acc);
+                mma_i8(tmem + 256, ai + o, b + o, kIdesc, acc);
+            }
+        }
+        tc_commit(smem_u32(bar));
+        if (!mbar_wait(smem_u32(bar), 0) && err) atomicOr(err, 2);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        tmem_dealloc(tmem, kTmemCols);
+    }
+}
+
 using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                               const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
                               const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -859,6 +910,23 @@ extern "C" int mixer_xcorr_tri_ex(const int8_t* planes, int32_t nant, int32_t nc
             mixer::xcorr_launch(planes, nant, nch, kt, kbeg + k, len, mode, vis, max_ctas, err, st);
         if (rc != MIXER_OK) return rc;
     }
+    return MIXER_OK;
+}
+
+extern "C" int mixer_mma_peak(int64_t iters, int32_t ctas, int32_t* err, void* stream) {
+    if (iters <= 0) return MIXER_EINVAL;
+    const int64_t n = ctas > 0 ? ctas : mixer::sm_count();
+    constexpr int smem = mixer::kStageBytes + 1024 + 64;
+    static uint64_t attr_set = 0;
+    int dev = 0;
+    MIXER_CK(cudaGetDevice(&dev));
+    if (dev < 64 && !(attr_set & (1ull << dev))) {
+        MIXER_CK(cudaFuncSetAttribute(mixer::k_mma_peak, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem));
+        attr_set |= 1ull << dev;
+    }
+    mixer::k_mma_peak<<<(unsigned)n, 128, smem, static_cast<cudaStream_t>(stream)>>>(iters, err);
+    MIXER_CK(cudaGetLastError());
     return MIXER_OK;
 }
 

@@ -101,6 +101,7 @@ _sig("mixer_corner_turn", C.c_int, _vp, _i64, _i32, _i32, _i32, _i32, _i32, _u32
      _vp, _vp, _vp)
 _sig("mixer_xcorr_tri", C.c_int, _vp, _i32, _i32, _i64, _i64, _i64, _i32, _vp, _vp, _vp)
 _sig("mixer_xcorr_tri_ex", C.c_int, _vp, _i32, _i32, _i64, _i64, _i64, _i32, _vp, _i32, _vp, _vp)
+_sig("mixer_mma_peak", C.c_int, _i64, _i32, _vp, _vp)
 _sig("mixer_vis_flush", C.c_int, _vp, _vp, _i64, _vp)
 _sig("mixer_vis_dump_f32", C.c_int, _vp, _i32, _i32, _vp, _vp)
 _sig("mixer_vis_unpack_i64", C.c_int, _vp, _i32, _i32, _vp, _vp)
@@ -154,7 +155,8 @@ _sig("mixer_shm_close", C.c_int, _vp, _i32)
 
 EXPORTED = [
     "mixer_vis_tiles", "mixer_vis_elems", "mixer_strerror", "mixer_device_ok",
-    "mixer_corner_turn", "mixer_xcorr_tri", "mixer_xcorr_tri_ex", "mixer_vis_flush", "mixer_vis_dump_f32",
+    "mixer_corner_turn", "mixer_xcorr_tri", "mixer_xcorr_tri_ex", "mixer_mma_peak",
+    "mixer_vis_flush", "mixer_vis_dump_f32",
     "mixer_vis_unpack_i64", "mixer_grid", "mixer_image_fft", "mixer_image_noalloc",
     "mixer_sky_table",
     "mixer_gen_packets", "mixer_desc_default", "mixer_create", "mixer_destroy", "mixer_reset",
@@ -230,6 +232,14 @@ def xcorr_tri(planes, nant, nch, kt, kbeg, klen, mode, vis, err=None, stream=Non
         return
     _check(_lib.mixer_xcorr_tri(_ptr(planes), nant, nch, kt, kbeg, klen, mode, _ptr(vis), _ptr(err),
                                 _stream(stream)), "mixer_xcorr_tri")
+
+
+def mma_peak(iters, ctas=0, err=None, stream=None):
+    """One launch of the tensor-core rate probe: iters x 8 int8 MMAs per CTA."""
+    _check(_lib.mixer_mma_peak(iters, ctas, _ptr(err), _stream(stream)), "mixer_mma_peak")
+
+
+MMA_PEAK_OPS_PER_ITER = 8 * 2 * 128 * 256 * 32   # per CTA and iteration
 
 
 def vis_flush(vis32, vis64, n, stream=None):

@@ -118,6 +118,14 @@ int mixer_xcorr_tri_ex(const int8_t* planes, int32_t nant, int32_t nch, int64_t 
                        int64_t kbeg, int64_t klen, int32_t mode, void* vis,
                        int32_t max_ctas, int32_t* err, void* stream);
 
+/* Tensor-core rate probe (no counterpart in the reference): `ctas` CTAs
+ * (<= 0: one per SM) each issue `iters` times the triangle GEMM's K-step (two
+ * M 128 x N 256 x K 32 int8 MMAs per 32 samples, four per 128-sample stage)
+ * from one resident shared-memory stage without any loads.  Each iteration is
+ * 8 MMAs of 2 x 128 x 256 x 32 ops: time it on `stream` for the dense int8
+ * rate the GEMM can approach on this device and clock.  err as above. */
+int mixer_mma_peak(int64_t iters, int32_t ctas, int32_t* err, void* stream);
+
 /* int32 -> int64 integration: vis64 += vis32; vis32 = 0 over n elements.
  * Replaces k_flush_cube (src/rx_host_corr.cu:90-95), which promotes into a
  * float cube and loses exactness past 2^24. */

@@ -243,6 +243,16 @@ def test_xcorr_partial_last_round_is_exact(cuda):
     assert np.array_equal(v64[:ref.size].cpu().numpy(), ref)
 
 
+def test_mma_peak_probe(cuda):
+    """The tensor-core rate probe runs its MMA stream to completion."""
+    import torch
+    err = _zeros(1, torch.int32, cuda)
+    mixer.mma_peak(200, 0, err)
+    mixer.mma_peak(50, 3, err)
+    _sync()
+    assert int(err.item()) == 0
+
+
 def test_xcorr_extreme_inputs(cuda):
     """-128 everywhere: exact here; the reference's -A_im (src/cgemm.cuh:52) wraps."""
     import torch
