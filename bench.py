@@ -38,9 +38,10 @@ SIGMA, SEED = 8.0, 20261203
 METRIC = "int8 cGEMM TOPS & input Gb/s vs roofline (stream vs plain); p50/p99 dump latency"
 L2_BYTES = 126 * 1024 * 1024
 # DRAM bytes of one k_xcorr_tri launch over its algorithmic bytes (planes read
-# once + int64 cube read and written), from the ncu capture of the N 1024,
-# C 64, K 4096 case: 1.6957 GB measured / 1.7456 GB algorithmic.
-XCORR_TRAFFIC_RATIO = 1.6957 / 1.7456
+# once + int64 cube read and written), from the ncu capture at the benchmark's
+# own K of 32 768 samples per launch on 1024 elements x 32 channels:
+# 2.7684 + 0.2753 GB measured / 2.7514 GB algorithmic (13 % extra plane reads).
+XCORR_TRAFFIC_RATIO = (2.7684 + 0.2753) / 2.7514
 
 
 # The plain (one array) workloads.  nch x tpkt = 4096 keeps the 8192-byte payload.
@@ -901,7 +902,8 @@ def run_ours(args):
                      "peak": peak, "unit": "TOPS", "frac": achieved / peak,
                      "peak_source": peak_src,
                      "traffic": XCORR_TRAFFIC_RATIO * (2 * NCH * NANT * kt + 2 * 8 * mixer.vis_elems(NANT, NCH)),
-                     "traffic_note": "bytes per launch, scaled from the ncu capture of a smaller case",
+                     "traffic_note": "bytes per launch: algorithmic x 1.106, the DRAM/algorithmic "
+                                     "ratio of an ncu capture at the same K (1024 el., 32 ch)",
                      "ops_per_launch": tri_ops(kt)},
         "clocks": clk.summary(),
         "gpu_launches": 2 * args.steps,
