@@ -62,25 +62,26 @@ __global__ void __launch_bounds__(256)
     const int total = 2 * nchg * V;
     const int64_t kcol = k0 + (int64_t)g * hg * tpkt;
     if (blockDim.x % V == 0) {
-        // Each thread keeps one column v of the rows and steps over (plane,
-        // channel) rows with additions only.
+        // Each thread keeps one column v of the rows and walks the channel rows
+        // of each plane with pointer increments only (no multiply per store).
         const int v = threadIdx.x % V;
         const int rstep = blockDim.x / V;
         const int kb = v * 16;
         const int hl = kb / tpkt;
-        const uint8_t* srow = sm + hl * hstride + (kb - hl * tpkt);
-        int8_t* dcol = planes + (int64_t)a * kt + kcol + kb;
         const int64_t cstride = (int64_t)nant * kt;   // one channel row to the next
-        int pc = threadIdx.x / V;
-        int plane = pc / nchg;
-        int cl = pc - plane * nchg;
-        for (; pc < 2 * nchg; pc += rstep) {
-            const uint4 val = *reinterpret_cast<const uint4*>(srow + plane * part + cl * tpkt);
-            *reinterpret_cast<uint4*>(dcol + ((int64_t)plane * nch + c0 + cl) * cstride) = val;
-            cl += rstep;
-            while (cl >= nchg) {
-                cl -= nchg;
-                ++plane;
+        const int64_t dstep = (int64_t)rstep * cstride;
+        const int sstep = rstep * tpkt;
+        const int cl0 = threadIdx.x / V;
+#pragma unroll 1
+        for (int plane = 0; plane < 2; ++plane) {
+            const uint8_t* src = sm + hl * hstride + (kb - hl * tpkt) + plane * part + cl0 * tpkt;
+            int8_t* dst = planes + ((int64_t)plane * nch + c0 + cl0) * cstride + (int64_t)a * kt +
+                          kcol + kb;
+#pragma unroll 4
+            for (int cl = cl0; cl < nchg; cl += rstep) {
+                *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(src);
+                src += sstep;
+                dst += dstep;
             }
         }
         return;
