@@ -243,6 +243,26 @@ def test_xcorr_partial_last_round_is_exact(cuda):
     assert np.array_equal(v64[:ref.size].cpu().numpy(), ref)
 
 
+@pytest.mark.parametrize("pairs", ["0", "1"])
+def test_xcorr_large_array_matches_oracle(cuda, monkeypatch, pairs):
+    """4096 elements (32 row blocks, 528 tiles per channel, tile indices past
+    the float decode's easy range) and 4000 (ragged last block), int64 mode,
+    one-SM and pair kernels."""
+    import torch
+    monkeypatch.setenv("MIXER_XCORR_PAIRS", pairs)
+    for nant in (4096, 4000):
+        rng = np.random.default_rng(nant)
+        nch, kt = 1, 384
+        planes = _rand_planes(rng, nch, nant, kt)
+        v64 = _zeros(mixer.vis_elems(nant, nch), torch.int64, cuda)
+        err = _zeros(1, torch.int32, cuda)
+        mixer.xcorr_tri(_t(planes, cuda), nant, nch, kt, 0, kt, mixer.VIS_ACC_I64, v64, err)
+        _sync()
+        assert int(err.item()) == 0
+        ref = oracle.vis_tile_pack(oracle.correlate(planes)).reshape(-1)
+        assert np.array_equal(v64.cpu().numpy(), ref), nant
+
+
 def test_mma_peak_probe(cuda):
     """The tensor-core rate probe runs its MMA stream to completion."""
     import torch
