@@ -213,6 +213,131 @@ __global__ void __launch_bounds__(512)
     }
 }
 
+// Warp-level form for G = 32, 64 or 128 (E = G / 32 values a lane).  A
+// length-G DIF FFT runs inside one warp: lane l holds elements x = l + 32 e;
+// stages of span h >= 32 pair values of the same lane, stages of span h < 32
+// pair lane l with lane l ^ h through shuffles, so no stage needs a block
+// barrier.  Rows first (grid rows read from global memory, coalesced), then
+// columns (from the padded shared-memory image, stride G + 1), both written
+// back in natural order (DIF leaves element x holding frequency bitrev(x));
+// then the shifted real part and the channel's max / min as above.
+template <int G>
+__device__ __forceinline__ void warp_fft(float2 (&v)[G / 32], const float2* __restrict__ tw, int lane) {
+    constexpr int E = G / 32;
+#pragma unroll
+    for (int h = G / 2; h >= 32; h >>= 1) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            if ((32 * e) & h) continue;                // upper element of its pair
+            const int e2 = e + h / 32;
+            const int j = (lane + 32 * e) & (2 * h - 1);
+            const float2 w = tw[j * (G / (2 * h))];
+            const float2 u = v[e], q = v[e2];
+            const float2 d = make_float2(u.x - q.x, u.y - q.y);
+            v[e] = make_float2(u.x + q.x, u.y + q.y);
+            v[e2] = make_float2(d.x * w.x - d.y * w.y, d.x * w.y + d.y * w.x);
+        }
+    }
+#pragma unroll
+    for (int h = 16; h >= 1; h >>= 1) {
+        const bool upper = (lane & h) != 0;
+        const float2 w = tw[(lane & (h - 1)) * (G / (2 * h))];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const float qx = __shfl_xor_sync(0xffffffffu, v[e].x, h);
+            const float qy = __shfl_xor_sync(0xffffffffu, v[e].y, h);
+            if (!upper) {
+                v[e] = make_float2(v[e].x + qx, v[e].y + qy);
+            } else {
+                const float2 d = make_float2(qx - v[e].x, qy - v[e].y);
+                v[e] = make_float2(d.x * w.x - d.y * w.y, d.x * w.y + d.y * w.x);
+            }
+        }
+    }
+}
+
+template <int G>
+__global__ void __launch_bounds__(1024)
+    k_image_fft_warp(const long long* __restrict__ grid, float* __restrict__ img,
+                     float* __restrict__ vmax, float* __restrict__ vmin) {
+    constexpr int E = G / 32, H = G / 2, P = G + 1, LOGG = G == 32 ? 5 : (G == 64 ? 6 : 7);
+    extern __shared__ float2 S[];                      // [G][G + 1] then twiddles [G / 2]
+    float2* tw = S + G * P;
+    __shared__ float red_max[32], red_min[32];
+    const int c = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    for (int k = threadIdx.x; k < H; k += blockDim.x) {
+        double sn, cs;
+        sincospi(2.0 * (double)k / (double)G, &sn, &cs);   // W_G^k = exp(-2 pi i k / G), FP64
+        tw[k] = make_float2((float)cs, (float)(-sn));
+    }
+    __syncthreads();
+    const long long* g = grid + (size_t)c * G * G * 2;
+    for (int y = warp; y < G; y += nwarps) {           // rows
+        float2 v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const longlong2 gv = reinterpret_cast<const longlong2*>(g)[y * G + lane + 32 * e];
+            v[e] = make_float2(__ll2float_rn(gv.x), __ll2float_rn(gv.y));
+        }
+        warp_fft<G>(v, tw, lane);
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+            S[y * P + (int)(__brev((unsigned)(lane + 32 * e)) >> (32 - LOGG))] = v[e];
+    }
+    __syncthreads();
+    for (int x = warp; x < G; x += nwarps) {           // columns
+        float2 v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = S[(lane + 32 * e) * P + x];
+        warp_fft<G>(v, tw, lane);
+        __syncwarp();
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+            S[(int)(__brev((unsigned)(lane + 32 * e)) >> (32 - LOGG)) * P + x] = v[e];
+    }
+    __syncthreads();
+    float mx = -3.4e38f, mn = 3.4e38f;
+    float* out = img + (size_t)c * G * G;
+    for (int q = threadIdx.x; q < G * G; q += blockDim.x) {
+        const int y = q / G, x = q - y * G;
+        const float v = S[((y + H) & (G - 1)) * P + ((x + H) & (G - 1))].x;
+        out[q] = v;
+        mx = fmaxf(mx, v);
+        mn = fminf(mn, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    }
+    if (lane == 0) {
+        red_max[warp] = mx;
+        red_min[warp] = mn;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < nwarps; ++w) {
+            mx = fmaxf(mx, red_max[w]);
+            mn = fminf(mn, red_min[w]);
+        }
+        if (vmax) vmax[c] = mx;
+        if (vmin) vmin[c] = mn;
+    }
+}
+
+template <int G>
+int launch_fft_warp(const int64_t* grid, int32_t nch, float* img, float* vmax, float* vmin,
+                    cudaStream_t st) {
+    const size_t smem = (size_t)G * (G + 1) * sizeof(float2) + (size_t)(G / 2) * sizeof(float2);
+    if (smem > 48 * 1024)
+        MIXER_CK(cudaFuncSetAttribute(k_image_fft_warp<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    k_image_fft_warp<G><<<(unsigned)nch, 1024, smem, st>>>(reinterpret_cast<const long long*>(grid),
+                                                           img, vmax, vmin);
+    MIXER_CK(cudaGetLastError());
+    return MIXER_OK;
+}
+
 }  // namespace
 }  // namespace mixer
 
@@ -259,6 +384,10 @@ extern "C" int mixer_image_fft(const int64_t* grid, int32_t nch, int32_t G, floa
     int logG = 0;
     while ((1 << logG) < G) ++logG;
     if ((1 << logG) != G || G < 4 || G > 128) return MIXER_EINVAL;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (G == 32) return mixer::launch_fft_warp<32>(grid, nch, img, vmax, vmin, st);
+    if (G == 64) return mixer::launch_fft_warp<64>(grid, nch, img, vmax, vmin, st);
+    if (G == 128) return mixer::launch_fft_warp<128>(grid, nch, img, vmax, vmin, st);
     const size_t smem = (size_t)G * G * sizeof(float2) + (size_t)(G / 2) * sizeof(float2);
     if (smem > 48 * 1024)
         MIXER_CK(cudaFuncSetAttribute(mixer::k_image_fft,
