@@ -20,6 +20,10 @@
 #include "common.cuh"
 
 namespace mixer {
+// Largest shared-memory window k_grid_tiles is launched with.
+constexpr size_t kGridSmemMax = 200 * 1024;
+size_t grid_smem_bytes(int nant, int side_x);
+
 namespace {
 
 __device__ __forceinline__ void decode_tile_g(int t, int& i, int& j) {
@@ -339,6 +343,20 @@ int launch_fft_warp(const int64_t* grid, int32_t nch, float* img, float* vmax, f
 }
 
 }  // namespace
+
+// Shared memory of k_grid_tiles: the largest baseline window of any tile
+// (16 bytes per int64 re / im cell).
+size_t grid_smem_bytes(int nant, int side_x) {
+    int maxcells = 0;
+    for (int i = 0; i * 128 < nant; ++i)
+        for (int j = 0; j <= i; ++j) {
+            int dylo, ny;
+            tile_window(i, j, nant, side_x, dylo, ny);
+            const int cells = ny * (2 * side_x - 1);
+            if (cells > maxcells) maxcells = cells;
+        }
+    return (size_t)maxcells * 16;
+}
 }  // namespace mixer
 
 extern "C" int mixer_grid(const int64_t* vis64, int32_t nant, int32_t nch, int32_t side_x,
@@ -347,16 +365,8 @@ extern "C" int mixer_grid(const int64_t* vis64, int32_t nant, int32_t nch, int32
     if (nch > 65535 || G > 4096) return MIXER_EINVAL;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int nt = mixer_vis_tiles(nant);
-    int maxcells = 0;
-    for (int t = 0, i = 0; i * 128 < nant; ++i)
-        for (int j = 0; j <= i; ++j, ++t) {
-            int dylo, ny;
-            mixer::tile_window(i, j, nant, side_x, dylo, ny);
-            const int cells = ny * (2 * side_x - 1);
-            if (cells > maxcells) maxcells = cells;
-        }
-    const size_t smem = (size_t)maxcells * 16;
-    if (smem > 200 * 1024) return MIXER_EINVAL;
+    const size_t smem = mixer::grid_smem_bytes(nant, side_x);
+    if (smem > mixer::kGridSmemMax) return MIXER_EINVAL;
     if (smem > 48 * 1024)
         MIXER_CK(cudaFuncSetAttribute(mixer::k_grid_tiles,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -427,8 +437,12 @@ int noalloc_grid_address(int64_t** out) {
 
 extern "C" int mixer_image_noalloc(const int64_t* vis64, int32_t nant, int32_t nch, int32_t side_x,
                                    int32_t G, float* img, float* vmax, float* vmin, void* stream) {
-    if (!vis64 || !img || nant <= 0 || nch <= 0 || side_x <= 0 || G <= 0) return MIXER_EINVAL;
+    // Every check of mixer_grid and mixer_image_fft is made here first, so a
+    // refused request enqueues nothing and leaves the shared array as it was.
+    if (!vis64 || !img || nant <= 0 || nch <= 0 || side_x <= 0) return MIXER_EINVAL;
+    if (G < 4 || G > 128 || (G & (G - 1)) != 0 || nch > 65535) return MIXER_EINVAL;
     if ((int64_t)nch * G * G > MIXER_NOALLOC_MAX_CELLS) return MIXER_EINVAL;
+    if (mixer::grid_smem_bytes(nant, side_x) > mixer::kGridSmemMax) return MIXER_EINVAL;
     int64_t* grid = nullptr;
     int rc = mixer::noalloc_grid_address(&grid);
     if (rc != MIXER_OK) return rc;

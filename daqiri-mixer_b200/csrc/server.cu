@@ -308,21 +308,41 @@ bool serve_once(mixer_server* sv) {
             continue;
         }
         DumpSlot& ds = s.dump[slot];
-        if (s.dump_copy_pending) cudaStreamWaitEvent(comp, s.ev_dump_copied, 0);
-        mixer_vis_dump_f32(s.vis, s.d.nant, s.d.nch, s.dump_dev, comp);
-        cudaMemsetAsync(s.vis, 0, (size_t)mixer_vis_elems(s.d.nant, s.d.nch) * 8, comp);
-        cudaEventRecord(s.ev_dump_kernel, comp);
-        cudaStreamWaitEvent(sv->d2h, s.ev_dump_kernel, 0);
+        s.subs_in_dump = 0;
+        // Every call of the dump edge is checked: on a failure the error is
+        // latched in sv->error (every later call reports it) and the slot stays
+        // free, so no poll can hand out a stale or partial cube.
         const size_t nbytes = (size_t)s.d.nch * 2 * s.d.nant * s.d.nant * sizeof(float);
-        cudaMemcpyAsync(ds.host, s.dump_dev, nbytes, cudaMemcpyDeviceToHost, sv->d2h);
-        cudaEventRecord(s.ev_dump_copied, sv->d2h);
+        cudaError_t e = cudaSuccess;
+        if (s.dump_copy_pending) e = cudaStreamWaitEvent(comp, s.ev_dump_copied, 0);
+        int drc = e == cudaSuccess ? mixer_vis_dump_f32(s.vis, s.d.nant, s.d.nch, s.dump_dev, comp)
+                                   : mixer::cuda_status(e, "dump edge: wait for the previous copy");
+        if (drc == MIXER_OK &&
+            ((e = cudaMemsetAsync(s.vis, 0, (size_t)mixer_vis_elems(s.d.nant, s.d.nch) * 8, comp)) !=
+                 cudaSuccess ||
+             (e = cudaEventRecord(s.ev_dump_kernel, comp)) != cudaSuccess ||
+             (e = cudaStreamWaitEvent(sv->d2h, s.ev_dump_kernel, 0)) != cudaSuccess ||
+             (e = cudaMemcpyAsync(ds.host, s.dump_dev, nbytes, cudaMemcpyDeviceToHost, sv->d2h)) !=
+                 cudaSuccess ||
+             (e = cudaEventRecord(s.ev_dump_copied, sv->d2h)) != cudaSuccess))
+            drc = mixer::cuda_status(e, "dump edge");
+        if (drc != MIXER_OK) {
+            sv->error.store(drc);
+            continue;
+        }
         s.dump_copy_pending = true;
+        ds.t_done.store(0.0);
+        DoneCtx* done = new DoneCtx{&ds};
+        if ((e = cudaLaunchHostFunc(sv->d2h, mark_done, done)) != cudaSuccess) {
+            delete done;
+            sv->error.store(mixer::cuda_status(e, "dump edge: completion callback"));
+            continue;
+        }
+        // sv->mu is held here and by collect_done, so the callback's time stamp
+        // is read only once the slot is marked in flight.
         ds.state = 1;
         ds.index = s.dumps_emitted++;
         ds.t_last_submit = s.t_slot_done[(s.subs_done - 1) % s.ring_subs];
-        ds.t_done.store(0.0);
-        cudaLaunchHostFunc(sv->d2h, mark_done, new DoneCtx{&ds});
-        s.subs_in_dump = 0;
     }
     return true;
 }
@@ -460,6 +480,10 @@ extern "C" int mixer_server_open(mixer_server* sv, const mixer_array_desc* d, in
         d->hdr_bytes % 16 || d->hdr_bytes < 64 ||
         (int64_t)d->hdr_bytes + 2LL * d->nch * d->tpkt > d->pkt_stride)
         return MIXER_EINVAL;
+    // Work items carry the tile index in 16 bits (at most 65535 lower-triangle
+    // tiles: nant <= 46208), and the channel limit of mixer_create holds here too.
+    const int64_t nblk = (d->nant + 127) / 128;
+    if (d->nant > 65536 || d->nch > 65535 || nblk * (nblk + 1) / 2 > 65535) return MIXER_EINVAL;
     const int64_t batch_subs = std::max<int64_t>(
         1, std::min<int64_t>(sv->cfg.batch_subs, MIXER_KMAX_I32 / d->ksub));
     const int64_t ring_subs = std::max<int64_t>(sv->cfg.ring_subs, 2);

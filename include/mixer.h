@@ -168,12 +168,19 @@ int mixer_image_fft(const int64_t* grid, int32_t nch, int32_t G, float* img,
  * receive loop where cudaMalloc / cudaFree could stall or synchronise the
  * device, or a host whose allocator belongs to another runtime.
  *   - Capacity: nch * G * G <= MIXER_NOALLOC_MAX_CELLS (16 MiB of int64 re/im
- *     cells, e.g. 256 x 64 x 64 or 64 x 128 x 128); larger requests return
- *     MIXER_EINVAL and touch nothing.
+ *     cells, e.g. 256 x 64 x 64 or 64 x 128 x 128).  Every request that
+ *     mixer_grid or mixer_image_fft would refuse (G not a power of two in
+ *     4..128, more than 65535 channels, an array too wide for the gridder's
+ *     shared-memory window) or that exceeds the capacity returns MIXER_EINVAL
+ *     before anything is enqueued: the shared array is left untouched.
  *   - The array is part of the library's device image, so every GPU that
  *     loads the library holds those 16 MiB until the process exits.
  *   - The first call on each device looks up the array's device address
- *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *     (cudaGetSymbolAddress) in that device's primary context, the one the
+ *     CUDA runtime uses, and keeps it for the life of the process; make that
+ *     first call before any stream capture.  Driving the device through
+ *     another driver-API context, or calling again after cudaDeviceReset, is
+ *     not supported: the kept address belongs to the first primary context.
  *   - All calls share the one array and it keeps the previous call's
  *     contents; each call clears it on `stream` before gridding.  Calls whose
  *     work overlaps on the GPU (different streams, or several host threads)

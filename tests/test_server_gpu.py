@@ -198,3 +198,21 @@ def test_server_poll_and_close_from_two_threads(cuda):
     st = srv.stats()
     assert st["kernel_err"] == 0 and st["bytes_used"] == 0
     srv.close()
+
+
+def test_server_refuses_oversize_descriptors(cuda):
+    """Admission refuses shapes the work list cannot address (more than 65535
+    lower-triangle tiles per channel, i.e. nant > 46208, or more than 65535
+    channels) before reserving anything, and the server stays usable."""
+    srv = mixer.Server(budget_bytes=1 << 40, max_streams=2, ring_subs=2, batch_subs=1)
+    for nant, nch in ((46209, 16), (1024, 65536)):
+        d = mixer.make_desc(nant=nant, nch=nch, tpkt=16, ksub=256, nsub_dump=1, side_x=16, grid=0,
+                            pkt_stride=64 + 2 * nch * 16, hdr_bytes=64, max_heaps=1)
+        with pytest.raises(mixer.MixerError) as e:
+            srv.open(d)
+        assert e.value.rc == mixer.EINVAL
+    assert srv.stats()["bytes_used"] == 0 and srv.stats()["admitted"] == 0
+    nant, nch, tpkt, ksub, nsub, side = STREAMS["B"]
+    sid = srv.open(_desc(nant, nch, tpkt, ksub, nsub, side))      # a valid shape still opens
+    srv.close_stream(sid)
+    srv.close()
