@@ -767,28 +767,65 @@ def serve_run(torch, mixer, kinds, pools, run_s, gbps, budget, jitter, rng):
     return out
 
 
-def serve_block(torch, mixer, dev, args, paced_s, unpaced_s, tight=False):
-    import numpy as np
-    rng = np.random.default_rng(SEED + 3)
-    kinds = ["256x128"] * 4 + ["1024x64"] * 4
-    pools = serve_pools(torch, mixer, dev, kinds)
+SERVE_BIN = os.path.join(ROOT, "daqiri-mixer_b200", "mixer_serve")
+
+
+def serve_cpp(seconds, gbps, budget_gb, jitter, device=0):
+    """One run of the C++ load generator (app/mixer_serve.cpp): eight feeder
+    threads on the C-ABI, one JSON line of results."""
+    if not os.path.exists(SERVE_BIN):
+        raise RuntimeError(f"{SERVE_BIN} missing: build it with make -C daqiri-mixer_b200")
+    cmd = [SERVE_BIN, "--seconds", str(seconds), "--gbps", str(gbps), "--budget-gb", str(budget_gb),
+           "--jitter", "1" if jitter else "0", "--device", str(device), "--seed", str(SEED)]
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=seconds + 300)
+    lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
+    if not lines:
+        raise RuntimeError(f"mixer_serve exited {p.returncode}: {p.stderr[-500:]}")
+    out = json.loads(lines[-1])
+    out["rc"] = p.returncode
+    period = {k: 1e3 * v[4] * (v[3] // v[2]) * v[0] * (64 + 2 * v[1] * v[2]) / (gbps / 8 * 1e9 / 8)
+              for k, v in SERVE_TYPES.items()} if gbps > 0 else None
+    if period:
+        out["integration_period_ms"] = period
+        out["p99_under_integration_period"] = out["p99_dump_latency_ms"] < min(period.values())
+    return out
+
+
+def serve_block(torch, mixer, dev, args, paced_s, unpaced_s, tight=False, python_feeders=False):
+    """Serving: the paced run (every stream at 380 / 8 Gb/s, Poisson-jittered
+    start / stop, budget for all eight), optionally the admission run with a
+    tight budget, and the unpaced run with all eight streams open from start to
+    end (the server's own ceiling).  C++ feeders (mixer_serve) unless
+    python_feeders."""
     out = {"workload": "8 streams: 4 x (256 elements x 128 ch, tpkt 32), 4 x (1024 elements x 64 ch, "
                        "tpkt 64), K 256, 64 sub-integrations per dump, 8256-byte heaps from the "
                        "seeded sky source (device pools), Poisson-jittered start / stop",
            "paced_gbps": args.serve_gbps, "budget_gb": args.serve_budget_full_gb}
-    out["paced"] = serve_run(torch, mixer, kinds, pools, paced_s, args.serve_gbps,
-                             int(args.serve_budget_full_gb * (1 << 30)), True, rng)
+    if python_feeders:
+        import numpy as np
+        rng = np.random.default_rng(SEED + 3)
+        kinds = ["256x128"] * 4 + ["1024x64"] * 4
+        pools = serve_pools(torch, mixer, dev, kinds)
+
+        def run(s, g, b, j):
+            return serve_run(torch, mixer, kinds, pools, s, g, int(b * (1 << 30)), j, rng)
+    else:
+        torch.cuda.empty_cache()
+
+        def run(s, g, b, j):
+            return serve_cpp(s, g, b, j, dev.index or 0)
+    out["paced"] = run(paced_s, args.serve_gbps, args.serve_budget_full_gb, True)
     if tight:
         out["tight_budget_gb"] = args.serve_budget_gb
-        out["paced_tight_budget"] = serve_run(torch, mixer, kinds, pools, paced_s, args.serve_gbps,
-                                              int(args.serve_budget_gb * (1 << 30)), True, rng)
+        out["paced_tight_budget"] = run(paced_s, args.serve_gbps, args.serve_budget_gb, True)
     if unpaced_s > 0:
-        out["unpaced_ceiling"] = serve_run(torch, mixer, kinds, pools, unpaced_s, 0.0, 64 << 30,
-                                           False, rng)
-    del pools
-    torch.cuda.empty_cache()
+        out["unpaced_ceiling"] = run(unpaced_s, 0.0, 64.0, False)
+    if python_feeders:
+        del pools
+        torch.cuda.empty_cache()
     runs = [v for k, v in out.items() if isinstance(v, dict) and "kernel_err" in v]
-    out["ok"] = all(r["kernel_err"] == 0 and r["seq_errors"] == 0 for r in runs)
+    out["ok"] = all(r["kernel_err"] == 0 and r["seq_errors"] == 0 and r.get("rc", 0) == 0
+                    for r in runs)
     return out
 
 
@@ -1203,8 +1240,8 @@ def run_serve(args):
     import mixer
     dev = torch.device("cuda:0")
     torch.cuda.set_device(dev)
-    out = serve_block(torch, mixer, dev, args, args.serve_seconds, min(args.serve_seconds, 6.0),
-                      tight=True)
+    out = serve_block(torch, mixer, dev, args, args.serve_seconds, min(args.serve_seconds, 10.0),
+                      tight=True, python_feeders=args.serve_python)
     print(json.dumps({"metric": "serving: sustained input Gb/s and p50/p99 dump latency", **out}))
     return 0 if out["ok"] else 1
 
@@ -1499,6 +1536,8 @@ def main():
     ap.add_argument("--serve-unpaced-seconds", type=float, default=5.0,
                     help="length of the unpaced serving run in the default line")
     ap.add_argument("--serve-gbps", type=float, default=380.0)
+    ap.add_argument("--serve-python", action="store_true",
+                    help="--config serve with Python feeder threads instead of mixer_serve")
     ap.add_argument("--serve-budget-gb", type=float, default=6.0,
                     help="device budget of the admission run (streams wait for memory)")
     ap.add_argument("--serve-budget-full-gb", type=float, default=16.0,
