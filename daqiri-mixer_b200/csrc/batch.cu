@@ -37,6 +37,7 @@ struct mixer_batch {
     int dev;
     std::vector<mixer_xcorr_problem> probs;
     std::vector<mixer::XcorrProblem> tprobs;
+    std::vector<char> shared_cube;     // per problem: its cube overlaps another problem's
     CUtensorMap* d_maps;
     mixer::XcorrProblem* d_probs;
     mixer::XcorrWork* d_work;
@@ -63,6 +64,9 @@ static int build_work(mixer_batch* b, std::vector<mixer::XcorrWork>& w) {
         if (pr.mode == MIXER_VIS_STORE_I32) s = 1;   // stores would race across items
         s = std::max<int64_t>(std::min<int64_t>(s, nkc), smin);
         const int64_t cs = (nkc + s - 1) / s;
+        // one item per (channel, tile) on a cube of its own: the epilogue may
+        // read-add-write instead of adding atomically
+        b->tprobs[p].excl = ((nkc + cs - 1) / cs == 1 && !b->shared_cube[p]) ? 1 : 0;
         for (int32_t c = 0; c < pr.nch; ++c)
             for (int t = 0; t < ntiles; ++t)
                 for (int64_t k0 = 0; k0 < nkc; k0 += cs) {
@@ -93,6 +97,8 @@ static int upload_plan(mixer_batch* b) {
         b->work_cap = (int64_t)w.size();
     }
     MIXER_CK(cudaMemcpy(b->d_work, w.data(), w.size() * sizeof(mixer::XcorrWork),
+                        cudaMemcpyHostToDevice));
+    MIXER_CK(cudaMemcpy(b->d_probs, b->tprobs.data(), b->tprobs.size() * sizeof(mixer::XcorrProblem),
                         cudaMemcpyHostToDevice));
     b->nwork = (int64_t)w.size();
     if (b->exec) {   // a captured graph refers to the old list
@@ -140,6 +146,20 @@ extern "C" int mixer_batch_create(const mixer_xcorr_problem* probs, int32_t npro
     int rc = MIXER_OK;
     std::vector<CUtensorMap> maps(nprob);
     b->tprobs.resize(nprob);
+    // problems whose cubes overlap share tiles: their items always add atomically
+    b->shared_cube.assign(nprob, 0);
+    for (int p = 0; p < nprob; ++p) {
+        const size_t es = probs[p].mode == MIXER_VIS_ACC_I64 ? 8 : 4;
+        const uintptr_t a0 = reinterpret_cast<uintptr_t>(probs[p].vis);
+        const uintptr_t a1 = a0 + (size_t)mixer_vis_elems(probs[p].nant, probs[p].nch) * es;
+        for (int q = 0; q < nprob; ++q) {
+            if (q == p) continue;
+            const size_t eq = probs[q].mode == MIXER_VIS_ACC_I64 ? 8 : 4;
+            const uintptr_t b0 = reinterpret_cast<uintptr_t>(probs[q].vis);
+            const uintptr_t b1 = b0 + (size_t)mixer_vis_elems(probs[q].nant, probs[q].nch) * eq;
+            if (a0 < b1 && b0 < a1) b->shared_cube[p] = 1;
+        }
+    }
     for (int p = 0; p < nprob && rc == MIXER_OK; ++p) {
         const mixer_xcorr_problem& q = probs[p];
         rc = mixer::xcorr_encode_map(&maps[p], q.planes, q.nant, q.nch, q.kt, q.kbeg + q.klen);

@@ -237,7 +237,9 @@ bool serve_once(mixer_server* sv) {
         const int mrc = mixer::xcorr_encode_map(&m, s.planes, s.d.nant, s.d.nch, s.kt, klen);
         if (mrc != MIXER_OK) sv->error.store(mrc);
         maps.push_back(m);
-        probs.push_back(mixer::XcorrProblem{s.d.nant, s.d.nch, ntiles, 0, MIXER_VIS_ACC_I64, 0, s.vis});
+        // one item per (channel, tile) over all ready sub-integrations, and every
+        // stream has a cube of its own: the items own their tiles
+        probs.push_back(mixer::XcorrProblem{s.d.nant, s.d.nch, ntiles, 0, MIXER_VIS_ACC_I64, 1, s.vis});
         for (int32_t c = 0; c < s.d.nch; ++c)
             for (int t = 0; t < ntiles; ++t) {
                 mixer::XcorrWork it;

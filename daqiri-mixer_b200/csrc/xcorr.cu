@@ -49,6 +49,11 @@ namespace {
 #ifndef MIXER_XCORR_EPI_GROUPS
 #define MIXER_XCORR_EPI_GROUPS 2
 #endif
+// int64 epilogue of an item that owns its tile: 1 = load, add, store; 0 = the
+// 64-bit atomic add used for shared tiles (K-split items) everywhere.
+#ifndef MIXER_XCORR_EXCL_RMW
+#define MIXER_XCORR_EXCL_RMW 1
+#endif
 constexpr int kTile = 128;                       // tile rows = cols
 constexpr int kWorkChunk = 128;                  // samples per work-list K unit
 constexpr int kKc = MIXER_XCORR_KC;              // samples (bytes) per pipeline stage
@@ -96,7 +101,7 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
 struct Item {
     const CUtensorMap* map;
     void* vis;
-    int c, t, i, j, kbeg, kc0, nkc, mode, ntiles;
+    int c, t, i, j, kbeg, kc0, nkc, mode, ntiles, excl;
 };
 
 __device__ __forceinline__ Item get_item(const XcorrArgs& a, const CUtensorMap* pmap, int64_t w) {
@@ -111,6 +116,7 @@ __device__ __forceinline__ Item get_item(const XcorrArgs& a, const CUtensorMap* 
         it.nkc = a.nkc;
         it.mode = a.mode;
         it.ntiles = a.ntiles;
+        it.excl = 1;          // one launch, one item per (channel, tile)
     } else {
         const XcorrWork wk = a.work[w];
         const XcorrProblem& pr = a.probs[wk.prob];
@@ -123,6 +129,7 @@ __device__ __forceinline__ Item get_item(const XcorrArgs& a, const CUtensorMap* 
         it.nkc = (int)wk.nkc;
         it.mode = pr.mode;
         it.ntiles = pr.ntiles;
+        it.excl = pr.excl;
     }
     decode_tile(it.t, it.i, it.j);
     return it;
@@ -316,7 +323,22 @@ __global__ void __launch_bounds__(kThreads, 1)
                     mbar_arrive(bar(ACCE));
                 }
                 const size_t e0 = tb + (size_t)(col0 + n0) * kTile + m;
-                if (it.mode == MIXER_VIS_ACC_I64) {
+                if (it.mode == MIXER_VIS_ACC_I64 && MIXER_XCORR_EXCL_RMW && it.excl) {
+                    // the item owns the tile: a warp reads, adds and writes 256
+                    // contiguous bytes per column and plane
+                    long long* v = reinterpret_cast<long long*>(it.vis) + e0;
+                    long long re[16], im[16];
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        re[e] = v[e * kTile];
+                        im[e] = v[e * kTile + kTile * kTile];
+                    }
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        v[e * kTile] = re[e] + (long long)(int32_t)(r[0][e] + r[3][e]);
+                        v[e * kTile + kTile * kTile] = im[e] + (long long)(int32_t)(r[2][e] - r[1][e]);
+                    }
+                } else if (it.mode == MIXER_VIS_ACC_I64) {
                     unsigned long long* v = reinterpret_cast<unsigned long long*>(it.vis) + e0;
 #pragma unroll
                     for (int e = 0; e < 16; ++e) {

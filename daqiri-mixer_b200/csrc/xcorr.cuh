@@ -5,10 +5,13 @@
 
 namespace mixer {
 
-// One array of a batched launch (device table entry).
+// One array of a batched launch (device table entry).  excl != 0 promises
+// that no other item of the launch adds into the same cube entries (one item
+// per tile and channel, and a cube no other array shares), so the int64
+// epilogue may read-add-write instead of using atomics.
 struct XcorrProblem {
     int32_t nant, nch, ntiles, kbeg;   // kbeg: first sample of the array's range
-    int32_t mode, pad_;
+    int32_t mode, excl;
     void* vis;
 };
 // One work item: array `prob`, channel `chan`, lower-triangle tile `tile`,
