@@ -559,7 +559,7 @@ def batched_block(torch, mixer, dev, S=4, small=False, rounds=5, reps=2, tune_re
     b = mixer.Batch(probs)
     t_untuned = timed(lambda: b.run(stream), 1)
     t0 = time.perf_counter()
-    tuned_ms = b.autotune(reps=tune_reps, stream=stream)
+    tuned_ms = b.autotune(reps=tune_reps, stream=stream) if tune_reps > 0 else None
     tune_s = time.perf_counter() - t0
     b.capture_graph(stream)
     # plain launches and the graph alternate, so the clock drift under the power
@@ -1527,7 +1527,8 @@ def main():
                     help="only the 1024-element workload (no small / large / batched / serve)")
     ap.add_argument("--batched-subints", type=int, default=4,
                     help="sub-integrations per array per batched pass")
-    ap.add_argument("--tune-reps", type=int, default=1, help="launches per autotuner sample")
+    ap.add_argument("--tune-reps", type=int, default=1,
+                    help="launches per autotuner sample (0: no autotuning, the default plan)")
     ap.add_argument("--nch", type=int, default=0,
                     help="channels per packet, tpkt = 4096/nch (0: the workload's)")
     ap.add_argument("--serve-seconds", type=float, default=30.0)
