@@ -4,7 +4,7 @@
 // samples per packet, four of 1024 elements x 64 channels with 64 samples per
 // packet; K 256 per sub-integration, a dump every 64 sub-integrations) are fed
 // to one mixer_server from eight C++ feeder threads, one per stream, each
-// replaying a device pool of one dump's worth of wire-format heaps from the
+// replaying a device pool of 64 sub-integrations of wire-format heaps from the
 // seeded packet source (the sequence numbers are re-stamped every lap so the
 // stream continues).  A poller thread takes the dumps as they complete.
 //
@@ -20,6 +20,10 @@
 // p99 / max dump latency and the server's counters.
 // Usage: mixer_serve [--seconds S] [--gbps R] [--budget-gb B] [--device D]
 //                    [--jitter 0|1] [--seed N] [--batch-subs N] [--ring-subs N]
+//                    [--nsub-dump N]
+// --nsub-dump N: sub-integrations per dump (default 64); the dump cubes cross
+// PCIe to host memory, so a sparser cadence shows how much of the unpaced
+// ceiling those copies take.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <atomic>
@@ -41,6 +45,7 @@ struct StreamType {
 };
 constexpr StreamType kTypes[2] = {{256, 128, 32, 256, 64, 16}, {1024, 64, 64, 256, 64, 32}};
 constexpr int kStreams = 8;
+constexpr int kPoolSubs = 64;      // sub-integrations of heaps in each replayed device pool
 
 double now_s() {
     using namespace std::chrono;
@@ -54,12 +59,13 @@ void sleep_s(double s) {
 struct Feed {
     StreamType ty;
     int64_t hps = 0, stride = 0, sub_bytes = 0;
-    uint8_t* pool = nullptr;       // nsub sub-integrations of heaps, device
+    uint8_t* pool = nullptr;       // kPoolSubs sub-integrations of heaps, device
     double start = 0, stop = 0;    // seconds from t0
     std::atomic<int> id{-1};
     int64_t submitted = 0, refusals = 0;
     double open_wait = 0, active = 0;
     std::vector<double> stamps;    // accepted submissions, seconds from t0
+    std::atomic<int64_t> dumps{0};  // dumps taken by the poller
     int err = MIXER_OK;
 };
 
@@ -67,7 +73,7 @@ struct Feed {
 
 int main(int argc, char** argv) {
     double seconds = 10.0, gbps = 380.0, budget_gb = 16.0;
-    int device = 0, jitter = 1, batch_subs = 8, ring_subs = 16;
+    int device = 0, jitter = 1, batch_subs = 8, ring_subs = 16, nsub_dump = 64;
     uint64_t seed = 20261203;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
@@ -80,9 +86,11 @@ int main(int argc, char** argv) {
         else if (a == "--seed") seed = strtoull(next(), nullptr, 10);
         else if (a == "--batch-subs") batch_subs = atoi(next());
         else if (a == "--ring-subs") ring_subs = atoi(next());
+        else if (a == "--nsub-dump") nsub_dump = atoi(next());
         else {
             fprintf(stderr, "usage: mixer_serve [--seconds S] [--gbps R] [--budget-gb B] [--device D] "
-                            "[--jitter 0|1] [--seed N] [--batch-subs N] [--ring-subs N]\n");
+                            "[--jitter 0|1] [--seed N] [--batch-subs N] [--ring-subs N] "
+                            "[--nsub-dump N]\n");
             return 2;
         }
     }
@@ -98,6 +106,7 @@ int main(int argc, char** argv) {
     for (int i = 0; i < kStreams; ++i) {
         Feed& f = feeds[i];
         f.ty = kTypes[i < 4 ? 0 : 1];
+        if (nsub_dump > 0) f.ty.nsub = nsub_dump;
         f.hps = f.ty.ksub / f.ty.tpkt;
         f.stride = 64 + 2LL * f.ty.nch * f.ty.tpkt;
         f.sub_bytes = f.hps * f.ty.nant * f.stride;
@@ -109,8 +118,8 @@ int main(int argc, char** argv) {
             f.start = 0;
             f.stop = seconds;
         }
-        // the pool: one dump of heaps of the star + planet sky, sigma 16
-        const int64_t nheaps = (int64_t)f.ty.nsub * f.hps;
+        // the pool: 64 sub-integrations of heaps of the star + planet sky, sigma 16
+        const int64_t nheaps = (int64_t)kPoolSubs * f.hps;
         if (cudaMalloc(&f.pool, (size_t)(nheaps * f.ty.nant * f.stride)) != cudaSuccess) {
             fprintf(stderr, "[mixer_serve] pool allocation failed\n");
             return 1;
@@ -189,10 +198,10 @@ int main(int argc, char** argv) {
         int64_t j = 0;
         bool stop = false;
         while (!stop && now_s() - t0 < f.stop) {
-            if (j % f.ty.nsub == 0) {        // new lap over the pool: re-stamp the sequence numbers
+            if (j % kPoolSubs == 0) {        // new lap over the pool: re-stamp the sequence numbers
                 int r = mixer_server_sync_copies(sv);      // the previous lap has been copied out
                 if (r == MIXER_OK)
-                    r = mixer_restamp_seq(f.pool, (int64_t)f.ty.nsub * f.hps * f.ty.nant, f.stride,
+                    r = mixer_restamp_seq(f.pool, (int64_t)kPoolSubs * f.hps * f.ty.nant, f.stride,
                                           (uint32_t)(j * f.hps * f.ty.nant), own);
                 if (r == MIXER_OK && cudaStreamSynchronize(own) != cudaSuccess) r = MIXER_ECUDA;
                 if (r != MIXER_OK) {
@@ -201,7 +210,7 @@ int main(int argc, char** argv) {
                 }
             }
             if (interval > 0) sleep_s(nxt - now_s());
-            const uint8_t* src = f.pool + (j % f.ty.nsub) * f.sub_bytes;
+            const uint8_t* src = f.pool + (j % kPoolSubs) * f.sub_bytes;
             while (true) {
                 const int r = mixer_server_submit(sv, sid, src, f.hps, 0, 1);
                 if (r == MIXER_OK) break;
@@ -236,8 +245,10 @@ int main(int argc, char** argv) {
                 const int sid = f.id.load();
                 if (sid < 0) continue;
                 mixer_dump_info info;
-                if (mixer_server_poll(sv, sid, &info, nullptr) == MIXER_OK && info.available)
+                if (mixer_server_poll(sv, sid, &info, nullptr) == MIXER_OK && info.available) {
                     polled.fetch_add(1);
+                    f.dumps.fetch_add(1);
+                }
             }
             sleep_s(0.001);
         }
@@ -270,6 +281,9 @@ int main(int argc, char** argv) {
     for (auto& f : feeds)
         for (double t : f.stamps)
             if (t >= w0 && t < w1) all_bytes += (double)f.sub_bytes;
+    double dump_bytes = 0;
+    for (auto& f : feeds)
+        dump_bytes += (double)f.dumps.load() * f.ty.nch * 2.0 * f.ty.nant * f.ty.nant * sizeof(float);
     int err = src;
     for (auto& f : feeds)
         if (f.err != MIXER_OK && err == MIXER_OK) err = f.err;
@@ -281,10 +295,11 @@ int main(int argc, char** argv) {
                8.0 * all_bytes / (w1 - w0) / 1e9);
     else
         printf("\"aggregate_while_all_streams_active\": null, ");
-    printf("\"dumps\": %lld, \"dumps_polled\": %lld, \"p50_dump_latency_ms\": %.3f, "
+    printf("\"dumps\": %lld, \"dumps_polled\": %lld, \"dump_d2h_gbytes_per_s\": %.2f, "
+           "\"sub_integrations_per_dump\": %d, \"p50_dump_latency_ms\": %.3f, "
            "\"p99_dump_latency_ms\": %.3f, \"max_dump_latency_ms\": %.3f, ",
-           (long long)st.dumps, (long long)polled.load(), 1e3 * st.p50_latency_s,
-           1e3 * st.p99_latency_s, 1e3 * st.max_latency_s);
+           (long long)st.dumps, (long long)polled.load(), dump_bytes / wall / 1e9, feeds[0].ty.nsub,
+           1e3 * st.p50_latency_s, 1e3 * st.p99_latency_s, 1e3 * st.max_latency_s);
     printf("\"per_stream_gbps\": [");
     for (int i = 0; i < kStreams; ++i)
         printf("%s%.1f", i ? ", " : "",
