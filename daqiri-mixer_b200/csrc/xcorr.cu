@@ -57,6 +57,14 @@ namespace {
 #ifndef MIXER_XCORR_EXCL_RMW
 #define MIXER_XCORR_EXCL_RMW 0
 #endif
+// Diagonal tiles (i == j) with three products instead of four: there
+// P1 = Xi Xr^T = P2^T, so one M 128 x N 256 MMA gives [R1 | P2], one
+// M 128 x N 128 MMA gives R2 = Xi Xi^T, and the epilogue forms
+// Im = P2^T - P2 by exchanging 32 x 32 blocks of P2 through shared memory.
+// 0: four products on every tile.
+#ifndef MIXER_XCORR_DIAG3
+#define MIXER_XCORR_DIAG3 1
+#endif
 constexpr int kTile = 128;                       // tile rows = cols
 constexpr int kWorkChunk = 128;                  // samples per work-list K unit
 constexpr int kKc = MIXER_XCORR_KC;              // samples (bytes) per pipeline stage
@@ -65,15 +73,25 @@ constexpr int kStages = MIXER_XCORR_STAGES;
 constexpr int kTileBytes = kTile * kKc;
 constexpr int kStageBytes = 4 * kTileBytes;      // Ar, Ai, Br, Bi
 static_assert(kKc == 64 || kKc == 128, "stage of 64 or 128 samples");
-static_assert(kStages * kStageBytes + 1024 + 256 <= 232448, "shared memory");
 constexpr int kEpiGroups = MIXER_XCORR_EPI_GROUPS;  // column groups per TMEM lane quadrant
 constexpr int kEpiWarps = 4 * kEpiGroups;
 constexpr int kEpiCols = kTile / kEpiGroups;     // 64 columns per warp
 constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr int kBarBytes = 256;
-constexpr int kSmemBytes = kStages * kStageBytes + 1024 + kBarBytes;
+// The diagonal-tile exchange needs the 2 x 4 layout of eight epilogue warps.
+constexpr bool kDiag3 = MIXER_XCORR_DIAG3 != 0 && kEpiGroups == 2;
+// Exchange area: one round's eight 32 x 32 int32 blocks of P2, rows padded to
+// 33 words so that both the row-wise writes and the column-wise reads of a
+// warp hit 32 different banks.
+constexpr int kXchgStride = 33;
+constexpr int kXchgBlock = 32 * kXchgStride;     // words per block
+constexpr int kXchgBytes = kDiag3 ? 8 * kXchgBlock * 4 : 0;
+constexpr int kSmemBytes = kStages * kStageBytes + 1024 + kBarBytes + kXchgBytes;
+static_assert(kSmemBytes <= 232448, "shared memory");
 constexpr uint32_t kTmemCols = 512;              // D1 (256) + D2 (256)
 constexpr uint32_t kIdesc = idesc_i8(128, 256);
+constexpr uint32_t kIdescN128 = idesc_i8(128, 128);
+constexpr int kEpiBarrier = 1;                   // named barrier of the eight epilogue warps
 
 struct XcorrArgs {
     int32_t nant, nch, nblk, ntiles;
@@ -169,6 +187,66 @@ __device__ __forceinline__ void tmem_ld4_x16(uint32_t a0, uint32_t a1, uint32_t 
         : "memory");
 }
 
+// One and three 32x32b.x16 TMEM loads (16 columns each) with their wait.
+__device__ __forceinline__ void tmem_ld_x16(uint32_t a, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(a)
+        : "memory");
+}
+
+__device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Adds (or stores) 16 columns of one row of a tile into the cube: element e at
+// e0 + e * 128 of the re plane and the im plane kTile * kTile further on.
+__device__ __forceinline__ void store16(const Item& it, size_t e0, const int32_t (&re)[16],
+                                        const int32_t (&im)[16]) {
+    if (it.mode == MIXER_VIS_ACC_I64 && MIXER_XCORR_EXCL_RMW && it.excl) {
+        // the item owns the tile: a warp reads, adds and writes 256 contiguous
+        // bytes per column and plane
+        long long* v = reinterpret_cast<long long*>(it.vis) + e0;
+        long long a[16], b[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            a[e] = v[e * kTile];
+            b[e] = v[e * kTile + kTile * kTile];
+        }
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            v[e * kTile] = a[e] + (long long)re[e];
+            v[e * kTile + kTile * kTile] = b[e] + (long long)im[e];
+        }
+    } else if (it.mode == MIXER_VIS_ACC_I64) {
+        unsigned long long* v = reinterpret_cast<unsigned long long*>(it.vis) + e0;
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            atomicAdd(v + e * kTile, (unsigned long long)(long long)re[e]);
+            atomicAdd(v + e * kTile + kTile * kTile, (unsigned long long)(long long)im[e]);
+        }
+    } else if (it.mode == MIXER_VIS_ACC_I32) {
+        int* v = reinterpret_cast<int*>(it.vis) + e0;
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            atomicAdd(v + e * kTile, re[e]);
+            atomicAdd(v + e * kTile + kTile * kTile, im[e]);
+        }
+    } else {
+        int* v = reinterpret_cast<int*>(it.vis) + e0;
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            v[e * kTile] = re[e];
+            v[e * kTile + kTile * kTile] = im[e];
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
     k_xcorr_tri(const __grid_constant__ CUtensorMap tmap, const XcorrArgs args) {
     extern __shared__ uint8_t smem_raw[];
@@ -178,6 +256,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + kStages * kStageBytes);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 4);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    int32_t* xchg = reinterpret_cast<int32_t*>(gbase + kStages * kStageBytes + kBarBytes);
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -273,12 +352,16 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const uint64_t ai = sdesc(sb + kTileBytes);
                     // 256-row B operand [Xr_j ; Xi_j]: two adjacent tiles
                     const uint64_t b = diag ? ar : sdesc(sb + 2 * kTileBytes);
+                    // diagonal tiles: D2 = Xi Xi^T (N 128) instead of Xi [Xr ; Xi]^T
+                    const bool three = kDiag3 && diag;
+                    const uint64_t b2 = three ? ai : b;
+                    const uint32_t id2 = three ? kIdescN128 : kIdesc;
 #pragma unroll
                     for (int kk = 0; kk < kKc / 32; ++kk) {
                         const uint64_t o = (uint64_t)((kk * 32) >> 4);   // 32-byte K step
                         const uint32_t acc = (kc > 0 || kk > 0) ? 1u : 0u;
                         mma_i8(t_d1, ar + o, b + o, kIdesc, acc);
-                        mma_i8(t_d2, ai + o, b + o, kIdesc, acc);
+                        mma_i8(t_d2, ai + o, b2 + o, id2, acc);
                     }
                     tc_commit(bar(EMPTY + stage));   // stage free once these MMAs finish
                     if (++stage == kStages) {
@@ -317,53 +400,72 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             tc_fence_after();
             const size_t tb = ((size_t)it.c * it.ntiles + it.t) * (size_t)(2 * kTile * kTile);
+            if (!(kDiag3 && it.i == it.j)) {
 #pragma unroll 1
-            for (int n0 = 0; n0 < kEpiCols; n0 += 16) {
-                uint32_t r[4][16];   // R1, P2, P1, R2
-                tmem_ld4_x16(trow + n0, trow + 128 + n0, trow + 256 + n0, trow + 384 + n0, r);
-                if (n0 == kEpiCols - 16) {           // this warp's TMEM reads are done
-                    tc_fence_before();
-                    mbar_arrive(bar(ACCE));
+                for (int n0 = 0; n0 < kEpiCols; n0 += 16) {
+                    uint32_t r[4][16];   // R1, P2, P1, R2
+                    tmem_ld4_x16(trow + n0, trow + 128 + n0, trow + 256 + n0, trow + 384 + n0, r);
+                    if (n0 == kEpiCols - 16) {           // this warp's TMEM reads are done
+                        tc_fence_before();
+                        mbar_arrive(bar(ACCE));
+                    }
+                    int32_t re[16], im[16];
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        re[e] = (int32_t)(r[0][e] + r[3][e]);
+                        im[e] = (int32_t)(r[2][e] - r[1][e]);
+                    }
+                    store16(it, tb + (size_t)(col0 + n0) * kTile + m, re, im);
                 }
-                const size_t e0 = tb + (size_t)(col0 + n0) * kTile + m;
-                if (it.mode == MIXER_VIS_ACC_I64 && MIXER_XCORR_EXCL_RMW && it.excl) {
-                    // the item owns the tile: a warp reads, adds and writes 256
-                    // contiguous bytes per column and plane
-                    long long* v = reinterpret_cast<long long*>(it.vis) + e0;
-                    long long re[16], im[16];
+            } else {
+                // Diagonal tile: TMEM holds R1 (columns 0-127), P2 (128-255) and
+                // R2 (256-383); Im[m][n] = P2[n][m] - P2[m][n].  Warp (q, h) owns
+                // rows 32q.. and columns 64h..; it needs P2[n][m] for n in its
+                // columns, i.e. the 32 x 32 blocks of P2 at rows of quadrants
+                // 2h, 2h+1 and columns 32q.., which the warps of those quadrants
+                // read from TMEM and pass through shared memory.  Round rho: the
+                // warps of quadrants 2rho, 2rho+1 write their blocks (slot =
+                // (quadrant - 2rho) * 4 + consumer quadrant), then the warps of
+                // column half rho read them transposed and write their rows.
+                const int hq = (warp - 2) >> 2;
+#pragma unroll 1
+                for (int rho = 0; rho < 2; ++rho) {
+                    if ((q >> 1) == rho) {
+#pragma unroll 1
+                        for (int g = 0; g < 4; ++g) {
+                            uint32_t p[16];
+                            tmem_ld_x16(trow + 128 + 16 * g, p);
+                            const int qc = 2 * hq + (g >> 1);
+                            int32_t* dst = xchg + ((q - 2 * rho) * 4 + qc) * kXchgBlock +
+                                           lane * kXchgStride + 16 * (g & 1);
 #pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        re[e] = v[e * kTile];
-                        im[e] = v[e * kTile + kTile * kTile];
+                            for (int e = 0; e < 16; ++e) dst[e] = (int32_t)p[e];
+                        }
                     }
+                    named_bar_sync(kEpiBarrier, 32 * kEpiWarps);
+                    if (hq == rho) {
+#pragma unroll 1
+                        for (int n0 = 0; n0 < kEpiCols; n0 += 16) {
+                            uint32_t r1[16], p2[16], r2[16];
+                            tmem_ld_x16(trow + n0, r1);
+                            tmem_ld_x16(trow + 128 + n0, p2);
+                            tmem_ld_x16(trow + 256 + n0, r2);
+                            int32_t re[16], im[16];
 #pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        v[e * kTile] = re[e] + (long long)(int32_t)(r[0][e] + r[3][e]);
-                        v[e * kTile + kTile * kTile] = im[e] + (long long)(int32_t)(r[2][e] - r[1][e]);
+                            for (int e = 0; e < 16; ++e) {
+                                const int ep = n0 + e;     // column within this warp's 64
+                                const int32_t p2t = xchg[((ep >> 5) * 4 + q) * kXchgBlock +
+                                                         (ep & 31) * kXchgStride + lane];
+                                re[e] = (int32_t)(r1[e] + r2[e]);
+                                im[e] = (int32_t)((uint32_t)p2t - p2[e]);
+                            }
+                            store16(it, tb + (size_t)(col0 + n0) * kTile + m, re, im);
+                        }
                     }
-                } else if (it.mode == MIXER_VIS_ACC_I64) {
-                    unsigned long long* v = reinterpret_cast<unsigned long long*>(it.vis) + e0;
-#pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        atomicAdd(v + e * kTile, (unsigned long long)(long long)(int32_t)(r[0][e] + r[3][e]));
-                        atomicAdd(v + e * kTile + kTile * kTile,
-                                  (unsigned long long)(long long)(int32_t)(r[2][e] - r[1][e]));
-                    }
-                } else if (it.mode == MIXER_VIS_ACC_I32) {
-                    int* v = reinterpret_cast<int*>(it.vis) + e0;
-#pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        atomicAdd(v + e * kTile, (int)(r[0][e] + r[3][e]));
-                        atomicAdd(v + e * kTile + kTile * kTile, (int)(r[2][e] - r[1][e]));
-                    }
-                } else {
-                    int* v = reinterpret_cast<int*>(it.vis) + e0;
-#pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        v[e * kTile] = (int)(r[0][e] + r[3][e]);
-                        v[e * kTile + kTile * kTile] = (int)(r[2][e] - r[1][e]);
-                    }
+                    named_bar_sync(kEpiBarrier, 32 * kEpiWarps);   // blocks consumed
                 }
+                tc_fence_before();
+                mbar_arrive(bar(ACCE));                 // every TMEM read of the tile done
             }
             acc_phase ^= 1u;
         }
