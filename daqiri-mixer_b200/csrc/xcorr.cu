@@ -63,7 +63,7 @@ namespace {
 // Im = P2^T - P2 by exchanging 32 x 32 blocks of P2 through shared memory.
 // 0: four products on every tile.
 #ifndef MIXER_XCORR_DIAG3
-#define MIXER_XCORR_DIAG3 1
+#define MIXER_XCORR_DIAG3 0
 #endif
 constexpr int kTile = 128;                       // tile rows = cols
 constexpr int kWorkChunk = 128;                  // samples per work-list K unit
