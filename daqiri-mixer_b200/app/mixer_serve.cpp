@@ -20,10 +20,13 @@
 // p99 / max dump latency and the server's counters.
 // Usage: mixer_serve [--seconds S] [--gbps R] [--budget-gb B] [--device D]
 //                    [--jitter 0|1] [--seed N] [--batch-subs N] [--ring-subs N]
-//                    [--nsub-dump N]
+//                    [--nsub-dump N] [--warm 0|1]
 // --nsub-dump N: sub-integrations per dump (default 64); the dump cubes cross
 // PCIe to host memory, so a sparser cadence shows how much of the unpaced
 // ceiling those copies take.
+// --warm 1: before the timed run, open and close every stream once, so the
+// server's device pool and pinned dump buffers already exist (a server that has
+// been running for a while); the first admissions then allocate nothing.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <atomic>
@@ -73,7 +76,7 @@ struct Feed {
 
 int main(int argc, char** argv) {
     double seconds = 10.0, gbps = 380.0, budget_gb = 16.0;
-    int device = 0, jitter = 1, batch_subs = 8, ring_subs = 16, nsub_dump = 64;
+    int device = 0, jitter = 1, batch_subs = 8, ring_subs = 16, nsub_dump = 64, warm = 0;
     uint64_t seed = 20261203;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
@@ -87,10 +90,11 @@ int main(int argc, char** argv) {
         else if (a == "--batch-subs") batch_subs = atoi(next());
         else if (a == "--ring-subs") ring_subs = atoi(next());
         else if (a == "--nsub-dump") nsub_dump = atoi(next());
+        else if (a == "--warm") warm = atoi(next());
         else {
             fprintf(stderr, "usage: mixer_serve [--seconds S] [--gbps R] [--budget-gb B] [--device D] "
                             "[--jitter 0|1] [--seed N] [--batch-subs N] [--ring-subs N] "
-                            "[--nsub-dump N]\n");
+                            "[--nsub-dump N] [--warm 0|1]\n");
             return 2;
         }
     }
@@ -153,13 +157,7 @@ int main(int argc, char** argv) {
         fprintf(stderr, "[mixer_serve] mixer_server_create: %s\n", mixer_strerror(rc));
         return 1;
     }
-    const double per_stream = gbps > 0 ? gbps / kStreams * 1e9 / 8 : 0.0;   // bytes / s
-    std::atomic<bool> done{false};
-    std::atomic<int64_t> polled{0};
-    const double t0 = now_s();
-
-    auto feeder = [&](int i) {
-        Feed& f = feeds[i];
+    auto desc_of = [&](const Feed& f) {
         mixer_array_desc d;
         mixer_desc_default(&d);
         d.nant = f.ty.nant;
@@ -172,6 +170,28 @@ int main(int argc, char** argv) {
         d.pkt_stride = (int32_t)f.stride;
         d.hdr_bytes = 64;
         d.max_heaps = 1;
+        return d;
+    };
+    if (warm) {
+        int ids[kStreams];
+        for (int i = 0; i < kStreams; ++i) {
+            const mixer_array_desc d = desc_of(feeds[i]);
+            rc = mixer_server_open(sv, &d, &ids[i]);
+            if (rc != MIXER_OK) {
+                fprintf(stderr, "[mixer_serve] warm-up open: %s\n", mixer_strerror(rc));
+                return 1;
+            }
+        }
+        for (int i = 0; i < kStreams; ++i) mixer_server_close(sv, ids[i]);
+    }
+    const double per_stream = gbps > 0 ? gbps / kStreams * 1e9 / 8 : 0.0;   // bytes / s
+    std::atomic<bool> done{false};
+    std::atomic<int64_t> polled{0};
+    const double t0 = now_s();
+
+    auto feeder = [&](int i) {
+        Feed& f = feeds[i];
+        const mixer_array_desc d = desc_of(f);
         cudaSetDevice(device);
         sleep_s(t0 + f.start - now_s());
         const double tw = now_s();
