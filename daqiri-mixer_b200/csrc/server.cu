@@ -44,8 +44,59 @@ double now_s() {
 
 constexpr int kDumpSlots = 2;
 
+// Pinned host memory in parts of at most kPinPart bytes.  Pinning a dump cube
+// (hundreds of MB) in one cudaMallocHost call keeps the driver busy long
+// enough to stall the other streams' launches and copies when a stream is
+// admitted; part by part, their calls get through in between.
+constexpr size_t kPinPart = (size_t)32 << 20;
+
+struct PinnedBuf {
+    std::vector<char*> parts;
+    size_t bytes = 0;
+    bool empty() const { return parts.empty(); }
+};
+
+void pinned_free(PinnedBuf& b) {
+    for (char* p : b.parts) cudaFreeHost(p);
+    b.parts.clear();
+    b.bytes = 0;
+}
+
+// All parts or none: a failed call leaves b empty.
+cudaError_t pinned_alloc(PinnedBuf& b, size_t bytes) {
+    b.bytes = bytes;
+    for (size_t off = 0; off < bytes; off += kPinPart) {
+        void* p = nullptr;
+        const cudaError_t e = cudaMallocHost(&p, std::min(kPinPart, bytes - off));
+        if (e != cudaSuccess) {
+            pinned_free(b);
+            return e;
+        }
+        b.parts.push_back(static_cast<char*>(p));
+        std::this_thread::yield();
+    }
+    return cudaSuccess;
+}
+
+// Device -> pinned host copy of `bytes`, one cudaMemcpyAsync per part.
+cudaError_t pinned_d2h(PinnedBuf& b, const void* src, size_t bytes, cudaStream_t st) {
+    const char* s = static_cast<const char*>(src);
+    for (size_t q = 0, off = 0; off < bytes; ++q, off += kPinPart) {
+        const cudaError_t e = cudaMemcpyAsync(b.parts[q], s + off, std::min(kPinPart, bytes - off),
+                                              cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+void pinned_read(const PinnedBuf& b, void* dst, size_t bytes) {
+    char* d = static_cast<char*>(dst);
+    for (size_t q = 0, off = 0; off < bytes; ++q, off += kPinPart)
+        memcpy(d + off, b.parts[q], std::min(kPinPart, bytes - off));
+}
+
 struct DumpSlot {
-    float* host = nullptr;          // pinned FP32 cube
+    PinnedBuf host;                 // pinned FP32 cube
     int state = 0;                  // 0 free, 1 in flight, 2 ready, 3 being read by poll
     int64_t index = 0;
     double t_last_submit = 0.0;
@@ -123,7 +174,10 @@ struct mixer_server {
     // other streams are being served.
     cudaMemPool_t pool = nullptr;
     cudaStream_t alloc = nullptr;
-    std::multimap<size_t, float*> pinned_cache;   // guarded by mu
+    std::multimap<size_t, PinnedBuf> pinned_cache;   // guarded by mu
+    // Superseded pinned work tables, freed with the server: cudaFreeHost would
+    // synchronise the device in the middle of serving.
+    std::vector<mixer::XcorrWork*> retired_work;
     std::thread worker;
     std::atomic<bool> stop{false};
     std::atomic<int> error{0};
@@ -161,7 +215,7 @@ void free_stream(mixer_server* sv, Stream& s) {
     if (s.ev_dump_kernel) cudaEventDestroy(s.ev_dump_kernel);
     const size_t dump_bytes = (size_t)s.d.nch * 2 * s.d.nant * s.d.nant * sizeof(float);
     for (auto& d : s.dump)
-        if (d.host) sv->pinned_cache.emplace(dump_bytes, d.host);
+        if (!d.host.empty()) sv->pinned_cache.emplace(dump_bytes, std::move(d.host));
     s.ring = nullptr;
     s.planes = nullptr;
     s.vis = nullptr;
@@ -172,7 +226,7 @@ void free_stream(mixer_server* sv, Stream& s) {
     s.ev_dump_copied = nullptr;
     s.ev_dump_kernel = nullptr;
     for (auto& d : s.dump) {
-        d.host = nullptr;
+        d.host = PinnedBuf();
         d.state = 0;
     }
     s.used = false;
@@ -259,13 +313,17 @@ bool serve_once(mixer_server* sv) {
     if (sv->table_used[ts]) cudaEventSynchronize(sv->table_free[ts]);
     const size_t np = probs.size();
     if ((int64_t)work.size() > sv->work_cap[ts]) {
-        cudaFree(sv->d_work[ts]);
-        cudaFreeHost(sv->h_work[ts]);
+        // grow without synchronising the device: the device table comes from the
+        // server's stream-ordered pool (the old one is released in stream order
+        // after its last launch), the old pinned table is kept until destroy
+        if (sv->d_work[ts]) cudaFreeAsync(sv->d_work[ts], comp);
+        if (sv->h_work[ts]) sv->retired_work.push_back(sv->h_work[ts]);
         sv->d_work[ts] = nullptr;
         sv->h_work[ts] = nullptr;
         sv->work_cap[ts] = 0;
         const size_t cap = work.size() + work.size() / 2;
-        cudaError_t e = cudaMalloc(&sv->d_work[ts], cap * sizeof(mixer::XcorrWork));
+        cudaError_t e = cudaMallocFromPoolAsync((void**)&sv->d_work[ts], cap * sizeof(mixer::XcorrWork),
+                                                sv->pool, comp);
         if (e == cudaSuccess) e = cudaMallocHost(&sv->h_work[ts], cap * sizeof(mixer::XcorrWork));
         if (e != cudaSuccess) {
             sv->error.store(mixer::cuda_status(e, "server work list"));
@@ -324,8 +382,7 @@ bool serve_once(mixer_server* sv) {
                  cudaSuccess ||
              (e = cudaEventRecord(s.ev_dump_kernel, comp)) != cudaSuccess ||
              (e = cudaStreamWaitEvent(sv->d2h, s.ev_dump_kernel, 0)) != cudaSuccess ||
-             (e = cudaMemcpyAsync(ds.host, s.dump_dev, nbytes, cudaMemcpyDeviceToHost, sv->d2h)) !=
-                 cudaSuccess ||
+             (e = pinned_d2h(ds.host, s.dump_dev, nbytes, sv->d2h)) != cudaSuccess ||
              (e = cudaEventRecord(s.ev_dump_copied, sv->d2h)) != cudaSuccess))
             drc = mixer::cuda_status(e, "dump edge");
         if (drc != MIXER_OK) {
@@ -426,6 +483,19 @@ extern "C" int mixer_server_create(const mixer_server_cfg* cfg, mixer_server** o
         if ((e = cudaMemPoolSetAttribute(sv->pool, cudaMemPoolAttrReleaseThreshold, &keep)) !=
             cudaSuccess)
             return fail(e, "server pool");
+        // Back the whole budget with device memory now, when it fits easily
+        // (at most half of the free memory): the first admissions then take it
+        // from the pool instead of mapping new memory while other streams run.
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && cfg->budget_bytes > 0 &&
+            (size_t)cfg->budget_bytes <= free_b / 2) {
+            void* p = nullptr;
+            if (cudaMallocFromPoolAsync(&p, (size_t)cfg->budget_bytes, sv->pool, sv->alloc) ==
+                cudaSuccess)
+                cudaFreeAsync(p, sv->alloc);
+            cudaGetLastError();        // a refused reservation only leaves the pool empty
+            if ((e = cudaStreamSynchronize(sv->alloc)) != cudaSuccess) return fail(e, "server pool");
+        }
     }
     for (int t = 0; t < 2; ++t) {
         if ((e = cudaMalloc(&sv->d_maps[t], cfg->max_streams * sizeof(CUtensorMap))) != cudaSuccess ||
@@ -453,14 +523,17 @@ extern "C" int mixer_server_destroy(mixer_server* sv) {
     if (sv->copy) cudaStreamSynchronize(sv->copy);
     for (int q = 0; q < sv->nstreams; ++q)
         if (sv->streams[q].used) free_stream(sv, sv->streams[q]);
+    for (int t = 0; t < 2; ++t)
+        if (sv->d_work[t] && sv->alloc) cudaFreeAsync(sv->d_work[t], sv->alloc);
     if (sv->alloc) cudaStreamSynchronize(sv->alloc);
     if (sv->pool) cudaMemPoolDestroy(sv->pool);
-    for (auto& kv : sv->pinned_cache) cudaFreeHost(kv.second);
+    for (auto& kv : sv->pinned_cache) pinned_free(kv.second);
     sv->pinned_cache.clear();
+    for (auto* p : sv->retired_work) cudaFreeHost(p);
+    sv->retired_work.clear();
     for (int t = 0; t < 2; ++t) {
         cudaFree(sv->d_maps[t]);
         cudaFree(sv->d_probs[t]);
-        cudaFree(sv->d_work[t]);
         cudaFreeHost(sv->h_maps[t]);
         cudaFreeHost(sv->h_probs[t]);
         cudaFreeHost(sv->h_work[t]);
@@ -538,11 +611,11 @@ extern "C" int mixer_server_open(mixer_server* sv, const mixer_array_desc* d, in
                 std::lock_guard<std::mutex> lk(sv->mu);
                 auto it = sv->pinned_cache.find(dump_bytes);
                 if (it != sv->pinned_cache.end()) {
-                    s.dump[q].host = it->second;
+                    s.dump[q].host = std::move(it->second);
                     sv->pinned_cache.erase(it);
                 }
             }
-            if (!s.dump[q].host) e = cudaMallocHost(&s.dump[q].host, dump_bytes);
+            if (s.dump[q].host.empty()) e = pinned_alloc(s.dump[q].host, dump_bytes);
         }
         s.ev_ready.assign(ring_subs, nullptr);
         s.ev_free.assign(ring_subs, nullptr);
@@ -645,7 +718,7 @@ extern "C" int mixer_server_poll(mixer_server* sv, int32_t id, mixer_dump_info* 
     }
     // the copy (hundreds of MB for a large array) runs without the server lock,
     // so the worker and the submitters are not held up by it
-    if (out) memcpy(out, best->host, nbytes);
+    if (out) pinned_read(best->host, out, nbytes);
     std::lock_guard<std::mutex> lk(sv->mu);
     best->state = 0;
     sp->readers -= 1;
