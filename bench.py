@@ -770,13 +770,16 @@ def serve_run(torch, mixer, kinds, pools, run_s, gbps, budget, jitter, rng):
 SERVE_BIN = os.path.join(ROOT, "daqiri-mixer_b200", "mixer_serve")
 
 
-def serve_cpp(seconds, gbps, budget_gb, jitter, device=0):
+def serve_cpp(seconds, gbps, budget_gb, jitter, device=0, reserve=True):
     """One run of the C++ load generator (app/mixer_serve.cpp): eight feeder
-    threads on the C-ABI, one JSON line of results."""
+    threads on the C-ABI, one JSON line of results.  reserve: the streams' state
+    is allocated before the run (mixer_server_reserve), as a server that knows
+    its stream shapes does at start-up."""
     if not os.path.exists(SERVE_BIN):
         raise RuntimeError(f"{SERVE_BIN} missing: build it with make -C daqiri-mixer_b200")
     cmd = [SERVE_BIN, "--seconds", str(seconds), "--gbps", str(gbps), "--budget-gb", str(budget_gb),
-           "--jitter", "1" if jitter else "0", "--device", str(device), "--seed", str(SEED)]
+           "--jitter", "1" if jitter else "0", "--device", str(device), "--seed", str(SEED),
+           "--reserve", "1" if reserve else "0"]
     p = subprocess.run(cmd, capture_output=True, text=True, timeout=seconds + 300)
     lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
     if not lines:
@@ -791,11 +794,14 @@ def serve_cpp(seconds, gbps, budget_gb, jitter, device=0):
     return out
 
 
-def serve_block(torch, mixer, dev, args, paced_s, unpaced_s, tight=False, python_feeders=False):
+def serve_block(torch, mixer, dev, args, paced_s, unpaced_s, tight=False, python_feeders=False,
+                cold=True):
     """Serving: the paced run (every stream at 380 / 8 Gb/s, Poisson-jittered
-    start / stop, budget for all eight), optionally the admission run with a
-    tight budget, and the unpaced run with all eight streams open from start to
-    end (the server's own ceiling).  C++ feeders (mixer_serve) unless
+    start / stop, budget for all eight, the streams' state reserved before the
+    run), the same run without the reservation (every admission allocates its
+    state while the other streams are served), optionally the admission run
+    with a tight budget, and the unpaced run with all eight streams open from
+    start to end (the server's own ceiling).  C++ feeders (mixer_serve) unless
     python_feeders."""
     out = {"workload": "8 streams: 4 x (256 elements x 128 ch, tpkt 32), 4 x (1024 elements x 64 ch, "
                        "tpkt 64), K 256, 64 sub-integrations per dump, 8256-byte heaps from the "
@@ -812,9 +818,12 @@ def serve_block(torch, mixer, dev, args, paced_s, unpaced_s, tight=False, python
     else:
         torch.cuda.empty_cache()
 
-        def run(s, g, b, j):
-            return serve_cpp(s, g, b, j, dev.index or 0)
+        def run(s, g, b, j, reserve=True):
+            return serve_cpp(s, g, b, j, dev.index or 0, reserve)
     out["paced"] = run(paced_s, args.serve_gbps, args.serve_budget_full_gb, True)
+    if cold and not python_feeders:
+        out["paced_cold_admission"] = run(paced_s, args.serve_gbps, args.serve_budget_full_gb, True,
+                                          reserve=False)
     if tight:
         out["tight_budget_gb"] = args.serve_budget_gb
         out["paced_tight_budget"] = run(paced_s, args.serve_gbps, args.serve_budget_gb, True)

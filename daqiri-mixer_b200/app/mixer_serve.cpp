@@ -20,13 +20,13 @@
 // p99 / max dump latency and the server's counters.
 // Usage: mixer_serve [--seconds S] [--gbps R] [--budget-gb B] [--device D]
 //                    [--jitter 0|1] [--seed N] [--batch-subs N] [--ring-subs N]
-//                    [--nsub-dump N] [--warm 0|1]
+//                    [--nsub-dump N] [--reserve 0|1]
 // --nsub-dump N: sub-integrations per dump (default 64); the dump cubes cross
 // PCIe to host memory, so a sparser cadence shows how much of the unpaced
 // ceiling those copies take.
-// --warm 1: before the timed run, open and close every stream once, so the
-// server's device pool and pinned dump buffers already exist (a server that has
-// been running for a while); the first admissions then allocate nothing.
+// --reserve 1: before the timed run, mixer_server_reserve allocates the state
+// of the eight streams (device pool, pinned dump buffers), as a server that
+// knows its stream shapes does at start-up; admissions then allocate nothing.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <atomic>
@@ -76,7 +76,7 @@ struct Feed {
 
 int main(int argc, char** argv) {
     double seconds = 10.0, gbps = 380.0, budget_gb = 16.0;
-    int device = 0, jitter = 1, batch_subs = 8, ring_subs = 16, nsub_dump = 64, warm = 0;
+    int device = 0, jitter = 1, batch_subs = 8, ring_subs = 16, nsub_dump = 64, reserve = 0;
     uint64_t seed = 20261203;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
@@ -90,11 +90,11 @@ int main(int argc, char** argv) {
         else if (a == "--batch-subs") batch_subs = atoi(next());
         else if (a == "--ring-subs") ring_subs = atoi(next());
         else if (a == "--nsub-dump") nsub_dump = atoi(next());
-        else if (a == "--warm") warm = atoi(next());
+        else if (a == "--reserve") reserve = atoi(next());
         else {
             fprintf(stderr, "usage: mixer_serve [--seconds S] [--gbps R] [--budget-gb B] [--device D] "
                             "[--jitter 0|1] [--seed N] [--batch-subs N] [--ring-subs N] "
-                            "[--nsub-dump N] [--warm 0|1]\n");
+                            "[--nsub-dump N] [--reserve 0|1]\n");
             return 2;
         }
     }
@@ -172,17 +172,15 @@ int main(int argc, char** argv) {
         d.max_heaps = 1;
         return d;
     };
-    if (warm) {
-        int ids[kStreams];
-        for (int i = 0; i < kStreams; ++i) {
-            const mixer_array_desc d = desc_of(feeds[i]);
-            rc = mixer_server_open(sv, &d, &ids[i]);
+    if (reserve) {
+        for (int t = 0; t < 2; ++t) {         // four streams of each of the two shapes
+            const mixer_array_desc d = desc_of(feeds[4 * t]);
+            rc = mixer_server_reserve(sv, &d, 4);
             if (rc != MIXER_OK) {
-                fprintf(stderr, "[mixer_serve] warm-up open: %s\n", mixer_strerror(rc));
+                fprintf(stderr, "[mixer_serve] mixer_server_reserve: %s\n", mixer_strerror(rc));
                 return 1;
             }
         }
-        for (int i = 0; i < kStreams; ++i) mixer_server_close(sv, ids[i]);
     }
     const double per_stream = gbps > 0 ? gbps / kStreams * 1e9 / 8 : 0.0;   // bytes / s
     std::atomic<bool> done{false};
@@ -307,9 +305,9 @@ int main(int argc, char** argv) {
     int err = src;
     for (auto& f : feeds)
         if (f.err != MIXER_OK && err == MIXER_OK) err = f.err;
-    printf("{\"feeders\": \"c++ threads (mixer_serve)\", \"wall_s\": %.3f, \"offered_gbps\": %.1f, "
-           "\"submitted_gbps\": %.2f, \"processed_gbps\": %.2f, ",
-           wall, gbps, 8.0 * total / wall / 1e9, 8.0 * (double)st.bytes_processed / wall / 1e9);
+    printf("{\"feeders\": \"c++ threads (mixer_serve)\", \"reserved\": %s, \"wall_s\": %.3f, "
+           "\"offered_gbps\": %.1f, \"submitted_gbps\": %.2f, \"processed_gbps\": %.2f, ",
+           reserve ? "true" : "false", wall, gbps, 8.0 * total / wall / 1e9, 8.0 * (double)st.bytes_processed / wall / 1e9);
     if (all_ran && w1 - w0 > 0.5)
         printf("\"aggregate_while_all_streams_active\": {\"window_s\": %.2f, \"gbps\": %.2f}, ", w1 - w0,
                8.0 * all_bytes / (w1 - w0) / 1e9);

@@ -450,6 +450,35 @@ extern "C" int64_t mixer_server_stream_bytes(const mixer_server_cfg* cfg, const 
     return stream_bytes(*d, ring_subs, batch_subs);
 }
 
+extern "C" int mixer_server_reserve(mixer_server* sv, const mixer_array_desc* d, int32_t count) {
+    if (!sv || !d || count < 0 || count > sv->nstreams) return MIXER_EINVAL;
+    if (d->nant <= 0 || d->nch <= 0 || d->nant > 65536 || d->nch > 65535) return MIXER_EINVAL;
+    const size_t dump_bytes = (size_t)d->nch * 2 * d->nant * d->nant * sizeof(float);
+    // device: take the streams' state from the pool once, so the pool holds it
+    const int64_t per = mixer_server_stream_bytes(&sv->cfg, d);
+    if (per <= 0) return MIXER_EINVAL;
+    std::vector<void*> blocks;
+    cudaError_t e = cudaSuccess;
+    for (int32_t i = 0; i < count && e == cudaSuccess; ++i) {
+        void* p = nullptr;
+        e = cudaMallocFromPoolAsync(&p, (size_t)per, sv->pool, sv->alloc);
+        if (e == cudaSuccess) blocks.push_back(p);
+    }
+    for (void* p : blocks) cudaFreeAsync(p, sv->alloc);
+    const cudaError_t es = cudaStreamSynchronize(sv->alloc);
+    if (e != cudaSuccess) return mixer::cuda_status(e, "mixer_server_reserve (device)");
+    if (es != cudaSuccess) return mixer::cuda_status(es, "mixer_server_reserve (device)");
+    // host: pinned dump buffers into the cache the admissions draw from
+    for (int32_t i = 0; i < count * kDumpSlots; ++i) {
+        PinnedBuf b;
+        if ((e = pinned_alloc(b, dump_bytes)) != cudaSuccess)
+            return mixer::cuda_status(e, "mixer_server_reserve (pinned)");
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->pinned_cache.emplace(dump_bytes, std::move(b));
+    }
+    return MIXER_OK;
+}
+
 extern "C" int mixer_server_create(const mixer_server_cfg* cfg, mixer_server** out) {
     if (!cfg || !out || cfg->budget_bytes <= 0 || cfg->max_streams <= 0 || cfg->max_streams > 4096)
         return MIXER_EINVAL;

@@ -132,6 +132,7 @@ _sig("mixer_server_create", C.c_int, C.POINTER(ServerCfg), C.POINTER(_vp))
 _sig("mixer_server_destroy", C.c_int, _vp)
 _sig("mixer_server_stream_bytes", _i64, C.POINTER(ServerCfg), C.POINTER(ArrayDesc))
 _sig("mixer_server_open", C.c_int, _vp, C.POINTER(ArrayDesc), C.POINTER(_i32))
+_sig("mixer_server_reserve", C.c_int, _vp, C.POINTER(ArrayDesc), _i32)
 _sig("mixer_server_close", C.c_int, _vp, _i32)
 _sig("mixer_server_submit", C.c_int, _vp, _i32, _vp, _i64, _u32, _i32)
 _sig("mixer_server_poll", C.c_int, _vp, _i32, C.POINTER(DumpInfo), _vp)
@@ -166,6 +167,7 @@ EXPORTED = [
     "mixer_batch_create", "mixer_batch_plan", "mixer_batch_autotune", "mixer_batch_run",
     "mixer_batch_capture_graph", "mixer_batch_replay", "mixer_batch_info", "mixer_batch_destroy",
     "mixer_server_create", "mixer_server_destroy", "mixer_server_stream_bytes", "mixer_server_open",
+    "mixer_server_reserve",
     "mixer_server_close", "mixer_server_submit", "mixer_server_poll", "mixer_server_stats",
     "mixer_server_sync_copies",
     "mixer_restamp_seq", "mixer_ctx_shape", "mixer_write_vis_i64", "mixer_state_save",
@@ -467,6 +469,11 @@ class Server:
 
     def stream_bytes(self, desc: ArrayDesc) -> int:
         return _lib.mixer_server_stream_bytes(C.byref(self.cfg), C.byref(desc))
+
+    def reserve(self, desc: ArrayDesc, count: int):
+        """Allocate the device and pinned host state of `count` streams of this
+        shape ahead of serving, so their admissions allocate nothing."""
+        _check(_lib.mixer_server_reserve(self._h, C.byref(desc), count), "mixer_server_reserve")
 
     def open(self, desc: ArrayDesc) -> int:
         sid = _i32()

@@ -365,6 +365,15 @@ int mixer_server_create(const mixer_server_cfg* cfg, mixer_server** out);
 int mixer_server_destroy(mixer_server* sv);
 /* Device bytes one stream of `d` reserves under `cfg`. */
 int64_t mixer_server_stream_bytes(const mixer_server_cfg* cfg, const mixer_array_desc* d);
+/* Allocation ahead of serving (no counterpart in the reference): device
+ * memory from the server's pool and the pinned host dump buffers for `count`
+ * streams of descriptor `d`, returned to the server's caches so that later
+ * admissions of that shape allocate nothing.  Pinning a dump cube takes on
+ * the order of a second per GB and holds the driver meanwhile, which delays
+ * the dumps of streams already being served; a server that knows its stream
+ * shapes reserves them before it starts.  Nothing counts against the budget
+ * until a stream is admitted.  Synchronous; count <= max_streams. */
+int mixer_server_reserve(mixer_server* sv, const mixer_array_desc* d, int32_t count);
 /* Admission: MIXER_EBUSY when the budget or the slots are exhausted. */
 int mixer_server_open(mixer_server* sv, const mixer_array_desc* d, int32_t* stream_id);
 /* Synchronises the server's streams, frees the stream's memory and slot. */

@@ -216,3 +216,42 @@ def test_server_refuses_oversize_descriptors(cuda):
     sid = srv.open(_desc(nant, nch, tpkt, ksub, nsub, side))      # a valid shape still opens
     srv.close_stream(sid)
     srv.close()
+
+
+def test_server_reserve_then_admit(cuda):
+    """mixer_server_reserve allocates streams' state ahead of serving; admissions
+    of that shape then succeed and their dumps are still exact; a reservation
+    for more streams than the server has slots is refused."""
+    import torch
+    nant, nch, tpkt, ksub, nsub, side = STREAMS["B"]
+    d = _desc(nant, nch, tpkt, ksub, nsub, side)
+    srv = mixer.Server(budget_bytes=8 << 30, max_streams=2, ring_subs=4, batch_subs=2)
+    with pytest.raises(mixer.MixerError) as e:
+        srv.reserve(d, 3)
+    assert e.value.rc == mixer.EINVAL
+    srv.reserve(d, 2)
+    assert srv.stats()["bytes_used"] == 0                 # nothing counts until admitted
+    pk = _packets("B", 1, seed=9)
+    want = _expected_dumps("B", pk, 1)[0]
+    dev = torch.from_numpy(pk).to(cuda)
+    hps = ksub // tpkt
+    hb = nant * (64 + 2 * nch * tpkt)
+    sids = [srv.open(d), srv.open(d)]
+    for sid in sids:
+        for q in range(nsub):
+            while not srv.submit(sid, dev[q * hps * hb:], hps, seq0=1000, on_device=True):
+                time.sleep(0.005)
+    buf = np.empty((nch, 2, nant, nant), dtype=np.float32)
+    for sid in sids:
+        t0 = time.time()
+        while True:
+            info = srv.poll(sid, buf)
+            if info is not None:
+                break
+            assert time.time() - t0 < 30, "no dump"
+            time.sleep(0.005)
+        assert np.array_equal(buf, want)
+        srv.close_stream(sid)
+    st = srv.stats()
+    assert st["kernel_err"] == 0 and st["seq_errors"] == 0 and st["bytes_used"] == 0
+    srv.close()
