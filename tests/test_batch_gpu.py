@@ -126,3 +126,44 @@ def test_batch_rejects_bad_problems(cuda):
         mixer.Batch([{"planes": pl, "nant": 128, "nch": 1, "kt": 100, "klen": 100,
                       "mode": mixer.VIS_ACC_I64, "vis": v}])
     assert e.value.rc == mixer.EINVAL
+
+
+@pytest.mark.parametrize("split", [1, 3])
+def test_batch_large_arrays_several_subintegrations(cuda, split):
+    """Arrays of the 48-array workload's sizes (N up to 1024, C up to 512), each
+    item contracting S = 4 sub-integrations of the array's K in one int32 TMEM
+    accumulation, against one mixer_xcorr_tri per array and sub-integration and
+    against the oracle on the first and last channel of every array.  With
+    split 3 the items share tiles (atomic epilogue); with split 1 each owns its
+    tile."""
+    import torch
+    S = 4
+    shapes = [(992, 352, 1024), (1024, 48, 512), (160, 512, 256), (608, 16, 1280)]   # (N, C, K)
+    g = torch.Generator(device=cuda).manual_seed(11)
+    probs, plain = [], []
+    for n, c, k in shapes:
+        planes = torch.randint(-127, 128, (2 * c * n * S * k,), dtype=torch.int8, device=cuda,
+                               generator=g)
+        probs.append({"planes": planes, "nant": n, "nch": c, "kt": S * k, "kbeg": 0, "klen": S * k,
+                      "mode": mixer.VIS_ACC_I64,
+                      "vis": torch.zeros(mixer.vis_elems(n, c), dtype=torch.int64, device=cuda)})
+        plain.append(torch.zeros(mixer.vis_elems(n, c), dtype=torch.int64, device=cuda))
+    for p, v in zip(probs, plain):
+        for s in range(S):
+            mixer.xcorr_tri(p["planes"], p["nant"], p["nch"], p["kt"], s * p["klen"] // S,
+                            p["klen"] // S, mixer.VIS_ACC_I64, v)
+    b = mixer.Batch(probs)
+    b.plan([split] * 65, mixer.ORDER_LPT)
+    b.run()
+    torch.cuda.synchronize()
+    assert b.info()["kernel_err"] == 0
+    for p, v in zip(probs, plain):
+        assert torch.equal(p["vis"], v), (p["nant"], p["nch"])
+        n, c = p["nant"], p["nch"]
+        per = mixer.vis_elems(n, 1)
+        for ch in (0, c - 1):
+            pl = p["planes"].view(2, c, n, -1)[:, ch:ch + 1].cpu().numpy()
+            want = oracle.vis_tile_pack(oracle.correlate(pl)).reshape(-1)
+            got = p["vis"][ch * per:(ch + 1) * per].cpu().numpy()
+            assert np.array_equal(got, want), (n, c, ch)
+    b.close()
