@@ -107,3 +107,61 @@ extern "C" int mixer_state_load(mixer_ctx* ctx, const char* path) {
     if (!ok) return MIXER_EINVAL;
     return mixer_write_vis_i64(ctx, host.data(), h.samples);
 }
+
+// ---- time-split multi-queue ingest ----------------------------------------------
+// The reference's sender steers snapshot (heap) tb to RX queue tb % MIXER_NQ through
+// the UDP destination port MIXER_UDP_PORT + q (src/config.h:40-45), so each queue
+// carries every nq-th heap.  The merge below restores time order on the host: heap
+// tb comes from queue tb % nq, must be the next heap at that queue's cursor, hold
+// nant packets with seqs tb * nant + a (a = 0 .. nant-1) and, when udp_port0 != 0,
+// carry destination port udp_port0 + q.  Heaps are copied to `out` until the first
+// one that is missing, incomplete, misordered or on the wrong port; every packet a
+// queue holds before its first aligned heap is skipped.  Integration is a sum over
+// samples, so the merged heaps give the same visibilities as one unsplit queue.
+extern "C" int mixer_merge_time_split(const uint8_t* const* queues, const int64_t* queue_npk,
+                                      int32_t nq, int64_t pkt_stride, int32_t nant,
+                                      uint16_t udp_port0, int64_t max_heaps, uint8_t* out,
+                                      int64_t* out_heaps, uint32_t* seq0, int64_t* consumed) {
+    if (!queues || !queue_npk || nq <= 0 || nq > 1024 || nant <= 0 ||
+        pkt_stride < MIXER_WIRE_SEQ_BYTE + 4 || max_heaps < 0 || !out_heaps || !consumed ||
+        (max_heaps > 0 && !out))
+        return MIXER_EINVAL;
+    for (int32_t q = 0; q < nq; ++q)
+        if (queue_npk[q] < 0 || (queue_npk[q] > 0 && !queues[q])) return MIXER_EINVAL;
+    auto seq = [&](int32_t q, int64_t p) { return seq_at(queues[q] + p * pkt_stride + MIXER_WIRE_SEQ_BYTE); };
+    auto port = [&](int32_t q, int64_t p) {
+        const uint8_t* h = queues[q] + p * pkt_stride;
+        return (uint16_t)((h[36] << 8) | h[37]);     // UDP destination port (eth 14 + ipv4 20 + 2)
+    };
+    // each queue's cursor: its first packet that starts a heap
+    std::vector<int64_t> cur(nq);
+    int64_t start_tb = -1;
+    for (int32_t q = 0; q < nq; ++q) {
+        int64_t p = 0;
+        while (p < queue_npk[q] && seq(q, p) % (uint32_t)nant != 0) ++p;
+        cur[q] = p;
+        if (p < queue_npk[q]) {
+            const int64_t tb = seq(q, p) / (uint32_t)nant;
+            if (start_tb < 0 || tb < start_tb) start_tb = tb;
+        }
+    }
+    *out_heaps = 0;
+    if (seq0) *seq0 = start_tb >= 0 ? (uint32_t)(start_tb * nant) : 0;
+    int64_t n = 0;
+    for (int64_t tb = start_tb; start_tb >= 0 && n < max_heaps; ++tb, ++n) {
+        const int32_t q = (int32_t)(tb % nq);
+        const int64_t p0 = cur[q];
+        if (p0 + nant > queue_npk[q]) break;                     // not (yet) complete
+        bool ok = true;
+        for (int32_t a = 0; a < nant && ok; ++a) {
+            ok = seq(q, p0 + a) == (uint32_t)(tb * nant + a) &&
+                 (udp_port0 == 0 || port(q, p0 + a) == (uint16_t)(udp_port0 + q));
+        }
+        if (!ok) break;
+        memcpy(out + n * nant * pkt_stride, queues[q] + p0 * pkt_stride, (size_t)(nant * pkt_stride));
+        cur[q] = p0 + nant;
+    }
+    *out_heaps = n;
+    for (int32_t q = 0; q < nq; ++q) consumed[q] = cur[q];
+    return MIXER_OK;
+}

@@ -125,6 +125,8 @@ _sig("mixer_ctx_shape", C.c_int, _vp, C.POINTER(_i32), C.POINTER(_i32))
 _sig("mixer_write_vis_i64", C.c_int, _vp, _vp, _i64)
 _sig("mixer_state_save", C.c_int, _vp, C.c_char_p)
 _sig("mixer_state_load", C.c_int, _vp, C.c_char_p)
+_sig("mixer_merge_time_split", C.c_int, C.POINTER(_vp), C.POINTER(_i64), _i32, _i64, _i32, _u16,
+     _i64, _vp, C.POINTER(_i64), C.POINTER(_u32), C.POINTER(_i64))
 _sig("mixer_align_heaps", C.c_int, _vp, _i64, _i64, _i32, C.POINTER(_i64), C.POINTER(_i64),
      C.POINTER(_i64), C.POINTER(_u32))
 _sig("mixer_desc_default", C.c_int, C.POINTER(ArrayDesc))
@@ -171,7 +173,7 @@ EXPORTED = [
     "mixer_server_close", "mixer_server_submit", "mixer_server_poll", "mixer_server_stats",
     "mixer_server_sync_copies",
     "mixer_restamp_seq", "mixer_ctx_shape", "mixer_write_vis_i64", "mixer_state_save",
-    "mixer_state_load", "mixer_align_heaps",
+    "mixer_state_load", "mixer_align_heaps", "mixer_merge_time_split",
 ]
 
 
@@ -298,6 +300,21 @@ def gen_packets(packets, pkt_stride, hdr_bytes, nant, nch, tpkt, nheaps, heap0, 
 def restamp_seq(packets, npk, pkt_stride, seq0, stream=None):
     _check(_lib.mixer_restamp_seq(_ptr(packets), npk, pkt_stride, seq0 & 0xFFFFFFFF, _stream(stream)),
            "mixer_restamp_seq")
+
+
+def merge_time_split(queues, pkt_stride, nant, udp_port0, max_heaps, out):
+    """Time-split multi-queue merge (host numpy buffers): queues = list of uint8
+    arrays of whole packets, heap tb in queue tb % len(queues).  Returns dict(heaps,
+    seq0, consumed=[packets used or skipped per queue])."""
+    nq = len(queues)
+    ptrs = (_vp * nq)(*[_ptr(q) for q in queues])
+    npk = (_i64 * nq)(*[q.size // pkt_stride for q in queues])
+    n, s0 = _i64(), _u32()
+    used = (_i64 * nq)()
+    _check(_lib.mixer_merge_time_split(ptrs, npk, nq, pkt_stride, nant, udp_port0, max_heaps,
+                                       _ptr(out), C.byref(n), C.byref(s0), used),
+           "mixer_merge_time_split")
+    return {"heaps": n.value, "seq0": s0.value, "consumed": list(used)}
 
 
 def align_heaps(packets, npk, pkt_stride, nant):

@@ -413,6 +413,22 @@ int mixer_state_load(mixer_ctx* ctx, const char* path);
 int mixer_align_heaps(const uint8_t* packets, int64_t npk, int64_t pkt_stride, int32_t nant,
                       int64_t* first, int64_t* nheaps, int64_t* next, uint32_t* seq0);
 
+/* Time-split multi-queue ingest (src/config.h:40-45, MIXER_NQ): the sender
+ * steers snapshot (heap) tb to RX queue q = tb % nq, UDP destination port
+ * MIXER_WIRE_UDP_PORT + q, so each queue's burst holds every nq-th heap in
+ * increasing tb.  Merges nq such bursts (host memory, `queue_npk[q]` packets
+ * each at `pkt_stride`) back into time order in `out` (host, room for
+ * max_heaps * nant packets): heap tb is taken from queue tb % nq and must be
+ * that queue's next heap, with seqs tb * nant + a and, when udp_port0 != 0,
+ * destination port udp_port0 + q.  The merge stops at the first heap that is
+ * missing, incomplete, misordered or on the wrong port.  *out_heaps = heaps
+ * written, *seq0 = seq of the first, consumed[q] = packets of queue q used or
+ * skipped (resume there).  The merged heaps go to mixer_correlate as one burst. */
+int mixer_merge_time_split(const uint8_t* const* queues, const int64_t* queue_npk, int32_t nq,
+                           int64_t pkt_stride, int32_t nant, uint16_t udp_port0,
+                           int64_t max_heaps, uint8_t* out, int64_t* out_heaps, uint32_t* seq0,
+                           int64_t* consumed);
+
 /* Corr32 shared-memory publisher (src/rx_host_corr.cu:97-105,236): header
  * {u32 magic 0x43523343, w, h, nch; u64 write_seq} then img[nch][G][G],
  * vmax[nch], vmin[nch].  name like "/corr32". */

@@ -107,3 +107,56 @@ def test_reference_viewer_reads_the_publication():
         shm.close()
     assert "channel 5/8" in out
     assert re.search(r"star peak \(x=20,y=9\)", out), out
+
+
+# ---- time-split multi-queue ingest (src/config.h:40-45, MIXER_NQ) -------------------
+
+def _split(nheaps, nq, seq0=0):
+    """One unsplit burst and its nq queues: heap tb goes to queue tb % nq, with the UDP
+    destination port 4096 + q written into its packets as the sender steers them."""
+    pk = _burst(nheaps, seq0=seq0).copy()
+    tb0 = seq0 // NANT
+    for h in range(nheaps):
+        q = (tb0 + h) % nq
+        rows = pk[h * NANT:(h + 1) * NANT]
+        rows[:, 36] = (4096 + q) >> 8
+        rows[:, 37] = (4096 + q) & 0xFF
+    queues = [np.ascontiguousarray(pk.reshape(nheaps, NANT, STRIDE)[[h for h in range(nheaps)
+                                                                      if (tb0 + h) % nq == q]])
+              .reshape(-1) for q in range(nq)]
+    return pk, queues
+
+
+@pytest.mark.parametrize("nq,seq0", [(1, 0), (2, 0), (4, 3 * NANT), (3, 5 * NANT)])
+def test_time_split_merge_restores_time_order(nq, seq0):
+    pk, queues = _split(12, nq, seq0)
+    out = np.zeros_like(pk).reshape(-1)
+    r = mixer.merge_time_split(queues, STRIDE, NANT, 4096, 64, out)
+    assert r["heaps"] == 12 and r["seq0"] == seq0
+    assert np.array_equal(out.reshape(pk.shape), pk)
+    assert r["consumed"] == [q.size // STRIDE for q in queues]
+
+
+def test_time_split_merge_stops_at_a_lost_heap():
+    nq = 3
+    pk, queues = _split(12, nq)
+    q1 = queues[1].reshape(-1, NANT, STRIDE)          # heaps 1, 4, 7, 10: lose heap 7
+    queues[1] = np.ascontiguousarray(np.delete(q1, 2, axis=0)).reshape(-1)
+    out = np.zeros_like(pk).reshape(-1)
+    r = mixer.merge_time_split(queues, STRIDE, NANT, 4096, 64, out)
+    assert r["heaps"] == 7                             # heaps 0..6, in order
+    assert np.array_equal(out.reshape(pk.shape)[:7 * NANT], pk[:7 * NANT])
+    assert r["consumed"] == [3 * NANT, 2 * NANT, 2 * NANT]
+
+
+def test_time_split_merge_checks_seq_and_port():
+    pk, queues = _split(8, 2)
+    bad = [q.copy() for q in queues]
+    bad[0].reshape(-1, STRIDE)[NANT + 3, 48:52] = 0xFF   # a corrupt seq inside heap 2 (queue 0)
+    out = np.zeros_like(pk).reshape(-1)
+    assert mixer.merge_time_split(bad, STRIDE, NANT, 4096, 64, out)["heaps"] == 2
+    bad = [q.copy() for q in queues]
+    bad[1].reshape(-1, STRIDE)[5, 37] ^= 1             # heap 1 arrived on another port
+    assert mixer.merge_time_split(bad, STRIDE, NANT, 4096, 64, out)["heaps"] == 1
+    assert mixer.merge_time_split(bad, STRIDE, NANT, 0, 64, out)["heaps"] == 8   # port unchecked
+    assert mixer.merge_time_split(queues, STRIDE, NANT, 4096, 3, out)["heaps"] == 3   # room for 3
