@@ -1340,6 +1340,8 @@ def run_ours(args):
                "d2h_bytes_per_step": int(NCH * G * G * 4 + 2 * NCH * 4),
                "ms_per_step": 1e3 * e2e_t / e2e_steps, "steps": e2e_steps,
                "ms_per_step_min_max": [min(per), max(per)],
+               "h2d_gbytes_per_s": e2e_npk * STRIDE * e2e_steps / e2e_t / 1e9,
+               "bound": "PCIe host-to-device copy of the packets (Gen5 x16, ~55 GB/s in practice)",
                "path": "mixer_correlate(host pinned packets) + mixer_image(host) per step"}
     del host
 
