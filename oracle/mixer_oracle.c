@@ -11,8 +11,9 @@
  *   - the correlator formula V = X X^H                   src/cgemm.cuh:4-7,58-63
  *       Re V[a][b] = sum xr_a xr_b + xi_a xi_b
  *       Im V[a][b] = sum xi_a xr_b - xr_a xi_b
- *     in exact int64 (OpenMP over channels and rows; int32 partial sums over
- *     blocks of <= 32768 samples, which cannot overflow);
+ *     in exact int64 (int32 partial sums over chunks of samples that cannot
+ *     overflow; the sum blocked over 2 x 4 pairs of rows widened to int16,
+ *     cross-checked against the pair-by-pair form orc_correlate_pairwise);
  *   - the gridding index map of k_grid_cube             src/rx_host_corr.cu:79-85
  *       every ordered pair (a, b): cell ((ya-yb) mod G, (xa-xb) mod G)
  *     summed exactly in int64;
@@ -215,12 +216,10 @@ static void dot4(const int8_t* xr_a, const int8_t* xi_a, const int8_t* xr_b, con
     *i_out = ir - ri;
 }
 
-/* Lower triangle of V for channels [c0, c0+nc) over samples [kbeg, kbeg+klen)
- * of planes [2][nch][nant][kt], ADDED into out[c - c0][2][nant][nant] at (a, b)
- * with b <= a; if mirror != 0 the upper triangle is then filled by
- * conjugation.  nthreads <= 0: OpenMP default. */
-int orc_correlate(const int8_t* planes, int nant, int nch, int64_t kt, int64_t kbeg, int64_t klen,
-                  int c0, int nc, int64_t* out, int mirror, int nthreads) {
+/* The formula pair by pair, one (a, b) at a time: the plain statement of the
+ * correlator, kept as the cross-check of the blocked one below. */
+int orc_correlate_pairwise(const int8_t* planes, int nant, int nch, int64_t kt, int64_t kbeg,
+                           int64_t klen, int c0, int nc, int64_t* out, int nthreads) {
     if (nthreads > 0) omp_set_num_threads(nthreads);
     const int64_t NN = (int64_t)nant * nant;
     const int64_t KB = 32768;
@@ -247,6 +246,106 @@ int orc_correlate(const int8_t* planes, int nant, int nch, int64_t kt, int64_t k
                 oim[b] += sim;
             }
         }
+    return 0;
+}
+
+/* One 2 x 4 block of (a, b) pairs over n int16 values (n / 2 samples).  Rows
+ * are (re, im) pairs, P_x = (xr, xi) and Q_x = (-xi, xr), so that
+ *   P_a . P_b = xr_a xr_b + xi_a xi_b = Re,   P_a . Q_b = xi_a xr_b - xr_a xi_b = Im
+ * and one widening multiply-add over adjacent int16 lanes gives a whole
+ * complex product's real or imaginary part.  The eight pairs share their row
+ * loads (2 + 8 rows for 16 sums instead of 4 rows per pair). */
+__attribute__((target_clones("arch=x86-64-v4", "arch=x86-64-v3", "default")))
+static void block2x4(const int16_t* restrict pa0, const int16_t* restrict pa1,
+                     const int16_t* restrict pb0, const int16_t* restrict pb1,
+                     const int16_t* restrict pb2, const int16_t* restrict pb3,
+                     const int16_t* restrict qb0, const int16_t* restrict qb1,
+                     const int16_t* restrict qb2, const int16_t* restrict qb3, int64_t n,
+                     int32_t re[8], int32_t im[8]) {
+    int32_t r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0, r5 = 0, r6 = 0, r7 = 0;
+    int32_t i0 = 0, i1 = 0, i2 = 0, i3 = 0, i4 = 0, i5 = 0, i6 = 0, i7 = 0;
+    for (int64_t j = 0; j < n; ++j) {
+        const int32_t a0 = pa0[j], a1 = pa1[j];
+        const int32_t b0 = pb0[j], b1 = pb1[j], b2 = pb2[j], b3 = pb3[j];
+        const int32_t q0 = qb0[j], q1 = qb1[j], q2 = qb2[j], q3 = qb3[j];
+        r0 += a0 * b0; r1 += a0 * b1; r2 += a0 * b2; r3 += a0 * b3;
+        r4 += a1 * b0; r5 += a1 * b1; r6 += a1 * b2; r7 += a1 * b3;
+        i0 += a0 * q0; i1 += a0 * q1; i2 += a0 * q2; i3 += a0 * q3;
+        i4 += a1 * q0; i5 += a1 * q1; i6 += a1 * q2; i7 += a1 * q3;
+    }
+    re[0] = r0; re[1] = r1; re[2] = r2; re[3] = r3; re[4] = r4; re[5] = r5; re[6] = r6; re[7] = r7;
+    im[0] = i0; im[1] = i1; im[2] = i2; im[3] = i3; im[4] = i4; im[5] = i5; im[6] = i6; im[7] = i7;
+}
+
+/* Lower triangle of V for channels [c0, c0+nc) over samples [kbeg, kbeg+klen)
+ * of planes [2][nch][nant][kt], ADDED into out[c - c0][2][nant][nant] at (a, b)
+ * with b <= a; if mirror != 0 the upper triangle is then filled by
+ * conjugation.  nthreads <= 0: OpenMP default.
+ * Blocked form of orc_correlate_pairwise (same sums, exactly): per channel and
+ * chunk of KC samples the rows are widened into P / Q (int16 pairs, rows padded
+ * with zeros to a multiple of 4) and the triangle is walked in 2 x 4 blocks of
+ * pairs; int32 partial sums per chunk (|sum| <= 2 * 128^2 * KC < 2^31) are
+ * added into int64. */
+int orc_correlate(const int8_t* planes, int nant, int nch, int64_t kt, int64_t kbeg, int64_t klen,
+                  int c0, int nc, int64_t* out, int mirror, int nthreads) {
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    const int64_t NN = (int64_t)nant * nant;
+    const int64_t KC = 1024;
+    const int npad = (nant + 3) & ~3;
+    const int64_t row = 2 * KC;                      /* int16 per row of a chunk */
+    int16_t* P = (int16_t*)calloc((size_t)npad * row, sizeof(int16_t));
+    int16_t* Q = (int16_t*)calloc((size_t)npad * row, sizeof(int16_t));
+    if (!P || !Q) {
+        free(P);
+        free(Q);
+        return -1;
+    }
+    for (int cc = 0; cc < nc; ++cc) {
+        const int c = c0 + cc;
+        int64_t* ore = out + (int64_t)cc * 2 * NN;
+        int64_t* oim = ore + NN;
+        for (int64_t k0 = kbeg; k0 < kbeg + klen; k0 += KC) {
+            const int64_t len = (k0 + KC < kbeg + klen) ? KC : kbeg + klen - k0;
+#pragma omp parallel for schedule(static)
+            for (int a = 0; a < npad; ++a) {
+                int16_t* p = P + (int64_t)a * row;
+                int16_t* q = Q + (int64_t)a * row;
+                if (a < nant) {
+                    const int8_t* xr = planes + ((int64_t)(0 * nch + c) * nant + a) * kt + k0;
+                    const int8_t* xi = planes + ((int64_t)(1 * nch + c) * nant + a) * kt + k0;
+                    for (int64_t k = 0; k < len; ++k) {
+                        p[2 * k] = xr[k];
+                        p[2 * k + 1] = xi[k];
+                        q[2 * k] = (int16_t)(-xi[k]);
+                        q[2 * k + 1] = xr[k];
+                    }
+                }
+                for (int64_t k = 2 * len; k < row; ++k) p[k] = q[k] = 0;
+            }
+#pragma omp parallel for schedule(dynamic, 1)
+            for (int a0 = 0; a0 < npad; a0 += 2) {
+                const int16_t* pa0 = P + (int64_t)a0 * row;
+                const int16_t* pa1 = pa0 + row;
+                for (int b0 = 0; b0 <= a0 + 1; b0 += 4) {
+                    const int16_t* pb = P + (int64_t)b0 * row;
+                    const int16_t* qb = Q + (int64_t)b0 * row;
+                    int32_t re[8], im[8];
+                    block2x4(pa0, pa1, pb, pb + row, pb + 2 * row, pb + 3 * row, qb, qb + row,
+                             qb + 2 * row, qb + 3 * row, 2 * len, re, im);
+                    for (int u = 0; u < 2; ++u)
+                        for (int v = 0; v < 4; ++v) {
+                            const int a = a0 + u, b = b0 + v;
+                            if (a < nant && b <= a) {
+                                ore[(int64_t)a * nant + b] += re[4 * u + v];
+                                oim[(int64_t)a * nant + b] += im[4 * u + v];
+                            }
+                        }
+                }
+            }
+        }
+    }
+    free(P);
+    free(Q);
     if (mirror) {
 #pragma omp parallel for schedule(static)
         for (int cc = 0; cc < nc; ++cc) {

@@ -40,6 +40,8 @@ def _load():
             ("orc_seq_errors", _i64, [_vp, _i64, _i64, _u32]),
             ("orc_correlate", C.c_int, [_vp, C.c_int, C.c_int, _i64, _i64, _i64, C.c_int, C.c_int,
                                         _vp, C.c_int, C.c_int]),
+            ("orc_correlate_pairwise", C.c_int, [_vp, C.c_int, C.c_int, _i64, _i64, _i64, C.c_int,
+                                                 C.c_int, _vp, C.c_int]),
             ("orc_grid", C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp]),
             ("orc_max_threads", C.c_int, []),
         ]:
@@ -102,6 +104,17 @@ def correlate(planes, kbeg=0, klen=None, c0=0, nc=None, out=None, mirror=True, n
         out = np.zeros((nc, 2, nant, nant), dtype=np.int64)
     _load().orc_correlate(_p(planes), nant, nch, kt, kbeg, klen, c0, nc, _p(out),
                           1 if mirror else 0, nthreads)
+    return out
+
+
+def correlate_pairwise(planes, kbeg=0, klen=None, c0=0, nc=None, nthreads=0):
+    """The same lower triangle as correlate(), one (a, b) pair at a time (the
+    plain statement of the formula, the cross-check of the blocked form)."""
+    _, nch, nant, kt = planes.shape
+    klen = kt - kbeg if klen is None else klen
+    nc = nch - c0 if nc is None else nc
+    out = np.zeros((nc, 2, nant, nant), dtype=np.int64)
+    _load().orc_correlate_pairwise(_p(planes), nant, nch, kt, kbeg, klen, c0, nc, _p(out), nthreads)
     return out
 
 

@@ -1,6 +1,7 @@
 """CPU checks of the oracle restatement against direct numpy statements of the
 reference formulas (src/cgemm.cuh:4-7, src/rx_host_corr.cu:63-71, :79-85)."""
 import numpy as np
+import pytest
 
 import oracle
 
@@ -108,3 +109,18 @@ def test_seq_error_count():
     stride = 64 + 2 * nch * tpkt
     pk.reshape(-1, stride)[10, 51] ^= 1    # corrupt one seq
     assert oracle.seq_errors(pk, 3 * nant, 5, stride) == 1
+
+
+@pytest.mark.parametrize("nant,nch,kt,kbeg,klen", [
+    (37, 3, 256, 0, 256), (130, 2, 5000, 16, 4960), (256, 1, 4096, 0, 4096), (5, 4, 48, 16, 32),
+])
+def test_blocked_correlator_equals_pairwise(nant, nch, kt, kbeg, klen):
+    """The blocked correlator (int16 pairs, 2 x 4 blocks, chunked int32 partial
+    sums) against the pair-by-pair statement of the formula, on full-range int8
+    including -128 and ragged shapes."""
+    rng = np.random.default_rng(nant * 7 + kt)
+    planes = rng.integers(-128, 128, size=(2, nch, nant, kt), dtype=np.int8)
+    planes[:, :, 0, :] = -128                          # the extreme row
+    got = oracle.correlate(planes, kbeg=kbeg, klen=klen, mirror=False)
+    want = oracle.correlate_pairwise(planes, kbeg=kbeg, klen=klen)
+    assert np.array_equal(got, want)
