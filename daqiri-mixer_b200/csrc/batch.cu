@@ -13,8 +13,11 @@
 // int64 read-modify-write epilogues per tile; integer sums are exact in any
 // order, so every split gives bit-identical visibilities.
 // Triangle schedule: items ordered longest-first (the static round-robin over
-// CTAs then approximates longest-processing-time scheduling) or in natural
-// array / channel / tile order (L2 locality of a channel's operands).
+// CTAs then approximates longest-processing-time scheduling), in natural
+// array / channel / tile order (L2 locality of a channel's operands), or with
+// the arrays interleaved channel by channel (a channel's tiles stay adjacent,
+// and CTAs working side by side hold items of different lengths, so their
+// int64 epilogues do not all reach DRAM at the same time).
 // The autotuner times candidate plans on the caller's own buffers, each in an
 // A-B-B-A pairing with the incumbent, and keeps a change only for a clear gain;
 // the chosen launch can be captured once into a CUDA graph and replayed.  This has no counterpart in the reference, which launches one
@@ -82,6 +85,10 @@ static int build_work(mixer_batch* b, std::vector<mixer::XcorrWork>& w) {
     if (b->order == MIXER_ORDER_LPT)
         std::stable_sort(w.begin(), w.end(), [](const mixer::XcorrWork& a, const mixer::XcorrWork& c) {
             return a.nkc > c.nkc;
+        });
+    else if (b->order == MIXER_ORDER_INTERLEAVE)   // channel 0 of every array, then channel 1, ...
+        std::stable_sort(w.begin(), w.end(), [](const mixer::XcorrWork& a, const mixer::XcorrWork& c) {
+            return a.chan < c.chan;
         });
     return MIXER_OK;
 }
@@ -192,7 +199,9 @@ extern "C" int mixer_batch_create(const mixer_xcorr_problem* probs, int32_t npro
 
 extern "C" int mixer_batch_plan(mixer_batch* b, const int32_t* split_per_class, int32_t nclass,
                                 int32_t order) {
-    if (!b || (order != MIXER_ORDER_LPT && order != MIXER_ORDER_CHANNEL)) return MIXER_EINVAL;
+    if (!b || (order != MIXER_ORDER_LPT && order != MIXER_ORDER_CHANNEL &&
+               order != MIXER_ORDER_INTERLEAVE))
+        return MIXER_EINVAL;
     if (nclass < 0 || nclass > kMaxClass + 1 || (nclass > 0 && !split_per_class)) return MIXER_EINVAL;
     for (int c = 0; c < nclass; ++c)
         if (split_per_class[c] < 1 || split_per_class[c] > 4096) return MIXER_EINVAL;
@@ -260,36 +269,39 @@ extern "C" int mixer_batch_autotune(mixer_batch* b, int32_t reps, void* stream, 
         if (work > 0.0) cls.push_back({work, c});
     }
     std::sort(cls.rbegin(), cls.rend());
-    int32_t plans[2][kMaxClass + 1];
-    const int orders[2] = {MIXER_ORDER_LPT, MIXER_ORDER_CHANNEL};
-    for (int o = 0; o < 2; ++o) {
-        int32_t* inc = plans[o];
-        for (int c = 0; c <= kMaxClass; ++c) inc[c] = 1;
-        for (const auto& wc : cls) {             // greedy K-split per class
-            const int c = wc.second;
-            for (int s : {2, 4, 8}) {
-                int32_t cand[kMaxClass + 1];
-                memcpy(cand, inc, sizeof(cand));
-                cand[c] = s;
-                float r;
-                const int rc = plan_ratio(b, inc, orders[o], cand, orders[o], reps, st, &r, nullptr);
-                if (rc != MIXER_OK) return rc;
-                if (r < kGain) inc[c] = s;       // keep a split only for a clear gain
-            }
+    // greedy K-split per size class, heaviest class first, with longest-first order
+    int32_t inc[kMaxClass + 1];
+    for (int c = 0; c <= kMaxClass; ++c) inc[c] = 1;
+    for (const auto& wc : cls) {
+        const int c = wc.second;
+        for (int s : {2, 4, 8}) {
+            int32_t cand[kMaxClass + 1];
+            memcpy(cand, inc, sizeof(cand));
+            cand[c] = s;
+            float r;
+            const int rc = plan_ratio(b, inc, MIXER_ORDER_LPT, cand, MIXER_ORDER_LPT, reps, st, &r, nullptr);
+            if (rc != MIXER_OK) return rc;
+            if (r < kGain) inc[c] = s;           // keep a split only for a clear gain
         }
     }
-    // the two orders' best plans against each other, then the winner against
-    // the default plan (longest-first, no split), which it must clearly beat
+    // then the item order with those splits: channel-major, then interleaved arrays
+    int best_order = MIXER_ORDER_LPT;
+    for (int o : {MIXER_ORDER_CHANNEL, MIXER_ORDER_INTERLEAVE}) {
+        float r;
+        const int rc = plan_ratio(b, inc, best_order, inc, o, reps, st, &r, nullptr);
+        if (rc != MIXER_OK) return rc;
+        if (r < kGain) best_order = o;
+    }
+    // the result against the default plan (longest-first, no split), which it must
+    // clearly beat
     float r;
-    int rc = plan_ratio(b, plans[0], orders[0], plans[1], orders[1], reps, st, &r, nullptr);
-    if (rc != MIXER_OK) return rc;
-    const int w = r < kGain ? 1 : 0;
+    int rc;
     int32_t dflt[kMaxClass + 1];
     for (int c = 0; c <= kMaxClass; ++c) dflt[c] = 1;
-    rc = plan_ratio(b, dflt, MIXER_ORDER_LPT, plans[w], orders[w], reps, st, &r, nullptr);
+    rc = plan_ratio(b, dflt, MIXER_ORDER_LPT, inc, best_order, reps, st, &r, nullptr);
     if (rc != MIXER_OK) return rc;
     if (r < kGain)
-        rc = mixer_batch_plan(b, plans[w], kMaxClass + 1, orders[w]);
+        rc = mixer_batch_plan(b, inc, kMaxClass + 1, best_order);
     else
         rc = mixer_batch_plan(b, dflt, kMaxClass + 1, MIXER_ORDER_LPT);
     if (rc == MIXER_OK && best_ms) rc = time_plan(b, reps, st, best_ms);
