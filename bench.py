@@ -601,7 +601,7 @@ def batched_block(torch, mixer, dev, S=4, small=False, rounds=5, reps=2, tune_re
         "input_gbps_plain": 8 * plane_bytes / t_plain / 1e6,
         "input_gbps_batched": 8 * plane_bytes / t_graph / 1e6,
         "autotune_s": tune_s, "autotune_best_ms": tuned_ms, "setup_s": gen_s,
-        "plan": {"nwork": info["nwork"], "order": ["lpt", "channel", "interleave"][info["order"]],
+        "plan": {"nwork": info["nwork"], "order": ["lpt", "channel"][info["order"]],
                  "split_per_class": {str(c): info["split"][c] for c in range(1, 9)}},
         "bit_exact_vs_plain": exact_vs_plain, "rounds": rounds, "reps": reps,
         "per_round_plain_over_graph": [round(x[0] / x[1], 3) for x in res],

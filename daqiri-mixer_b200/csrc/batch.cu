@@ -13,11 +13,8 @@
 // int64 read-modify-write epilogues per tile; integer sums are exact in any
 // order, so every split gives bit-identical visibilities.
 // Triangle schedule: items ordered longest-first (the static round-robin over
-// CTAs then approximates longest-processing-time scheduling), in natural
-// array / channel / tile order (L2 locality of a channel's operands), or with
-// the arrays interleaved channel by channel (a channel's tiles stay adjacent,
-// and CTAs working side by side hold items of different lengths, so their
-// int64 epilogues do not all reach DRAM at the same time).
+// CTAs then approximates longest-processing-time scheduling) or in natural
+// array / channel / tile order (L2 locality of a channel's operands).
 // The autotuner times candidate plans on the caller's own buffers, each in an
 // A-B-B-A pairing with the incumbent, and keeps a change only for a clear gain;
 // the chosen launch can be captured once into a CUDA graph and replayed.  This has no counterpart in the reference, which launches one
@@ -86,10 +83,7 @@ static int build_work(mixer_batch* b, std::vector<mixer::XcorrWork>& w) {
         std::stable_sort(w.begin(), w.end(), [](const mixer::XcorrWork& a, const mixer::XcorrWork& c) {
             return a.nkc > c.nkc;
         });
-    else if (b->order == MIXER_ORDER_INTERLEAVE)   // channel 0 of every array, then channel 1, ...
-        std::stable_sort(w.begin(), w.end(), [](const mixer::XcorrWork& a, const mixer::XcorrWork& c) {
-            return a.chan < c.chan;
-        });
+
     return MIXER_OK;
 }
 
@@ -199,9 +193,7 @@ extern "C" int mixer_batch_create(const mixer_xcorr_problem* probs, int32_t npro
 
 extern "C" int mixer_batch_plan(mixer_batch* b, const int32_t* split_per_class, int32_t nclass,
                                 int32_t order) {
-    if (!b || (order != MIXER_ORDER_LPT && order != MIXER_ORDER_CHANNEL &&
-               order != MIXER_ORDER_INTERLEAVE))
-        return MIXER_EINVAL;
+    if (!b || (order != MIXER_ORDER_LPT && order != MIXER_ORDER_CHANNEL)) return MIXER_EINVAL;
     if (nclass < 0 || nclass > kMaxClass + 1 || (nclass > 0 && !split_per_class)) return MIXER_EINVAL;
     for (int c = 0; c < nclass; ++c)
         if (split_per_class[c] < 1 || split_per_class[c] > 4096) return MIXER_EINVAL;
@@ -284,13 +276,13 @@ extern "C" int mixer_batch_autotune(mixer_batch* b, int32_t reps, void* stream, 
             if (r < kGain) inc[c] = s;           // keep a split only for a clear gain
         }
     }
-    // then the item order with those splits: channel-major, then interleaved arrays
+    // then the channel-major order with those splits
     int best_order = MIXER_ORDER_LPT;
-    for (int o : {MIXER_ORDER_CHANNEL, MIXER_ORDER_INTERLEAVE}) {
+    {
         float r;
-        const int rc = plan_ratio(b, inc, best_order, inc, o, reps, st, &r, nullptr);
+        const int rc = plan_ratio(b, inc, MIXER_ORDER_LPT, inc, MIXER_ORDER_CHANNEL, reps, st, &r, nullptr);
         if (rc != MIXER_OK) return rc;
-        if (r < kGain) best_order = o;
+        if (r < kGain) best_order = MIXER_ORDER_CHANNEL;
     }
     // the result against the default plan (longest-first, no split), which it must
     // clearly beat

@@ -59,7 +59,7 @@ class XcorrProblem(C.Structure):
                 ("klen", _i64), ("mode", _i32), ("vis", _vp)]
 
 
-ORDER_LPT, ORDER_CHANNEL, ORDER_INTERLEAVE = 0, 1, 2
+ORDER_LPT, ORDER_CHANNEL = 0, 1
 
 
 class ServerCfg(C.Structure):

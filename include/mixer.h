@@ -229,7 +229,6 @@ typedef struct mixer_batch mixer_batch;
 
 #define MIXER_ORDER_LPT     0   /* items longest first (longest-processing-time) */
 #define MIXER_ORDER_CHANNEL 1   /* array, channel, tile order (L2 locality)       */
-#define MIXER_ORDER_INTERLEAVE 2 /* channel 0 of every array, then channel 1, ...  */
 
 /* Many independent arrays of different N, C and K in ONE persistent launch of
  * the triangle cGEMM (no counterpart in the reference, which launches one
@@ -242,7 +241,7 @@ int mixer_batch_create(const mixer_xcorr_problem* probs, int32_t nprob, mixer_ba
  * index 0..nclass-1) and item order. */
 int mixer_batch_plan(mixer_batch* b, const int32_t* split_per_class, int32_t nclass, int32_t order);
 /* Autotuner: times candidate plans on the caller's own buffers -- a greedy
- * per-class K-split with longest-first order, then the other two orders with
+ * per-class K-split with longest-first order, then channel-major order with
  * that split -- `reps` launches per sample, each candidate against the
  * incumbent in an A-B-B-A pairing (clock drift cancels); a change is kept only
  * when it is at least 2 % faster, and the result must beat the default plan

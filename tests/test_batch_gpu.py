@@ -48,7 +48,6 @@ def _zero(probs):
 @pytest.mark.parametrize("split,order", [
     ([1] * 65, mixer.ORDER_LPT), ([1] * 65, mixer.ORDER_CHANNEL),
     ([3] * 65, mixer.ORDER_LPT), ([1, 2, 4, 8, 16] + [1] * 60, mixer.ORDER_CHANNEL),
-    ([1] * 65, mixer.ORDER_INTERLEAVE), ([2] * 65, mixer.ORDER_INTERLEAVE),
 ])
 def test_batch_plans_bit_exact(cuda, split, order):
     probs = _problems(cuda)
