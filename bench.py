@@ -503,6 +503,15 @@ def batched_block(torch, mixer, dev, S=4, small=False, rounds=5, reps=2, tune_re
     and the sampled arrays' V go to the CPU leg for the oracle check."""
     stream = torch.cuda.Stream()
     arrays = batched_arrays(small=small)
+    # the largest S up to the one asked for whose planes, cubes and packet buffer fit
+    # in 90 % of the free device memory
+    free, _ = torch.cuda.mem_get_info(dev)
+    per_sub = sum(2 * n * c * k for n, c, k, _, _ in arrays)
+    cubes = sum(8 * mixer.vis_elems(n, c) for n, c, _, _, _ in arrays)
+    pk_max = max((k // 16) * n * (64 + 32 * c) for n, c, k, _, _ in arrays)
+    S_asked = S
+    while S > 1 and S * per_sub + cubes + pk_max > 0.9 * free:
+        S -= 1
     probs, total_ops, plane_bytes = [], 0.0, 0
     t_gen = time.perf_counter()
     for idx, (n, c, k, l, m) in enumerate(arrays):
@@ -593,7 +602,8 @@ def batched_block(torch, mixer, dev, S=4, small=False, rounds=5, reps=2, tune_re
                      "48 arrays, N in {64..1024 step 32}, C in {16..512 step 16}")
         + f", K in {{256..4096 step 256}} per sub-integration, {S} sub-integrations per pass, "
           "1 source + sigma 12 noise each (seeded)",
-        "subints_per_pass": S, "total_ops": total_ops, "plane_bytes": plane_bytes,
+        "subints_per_pass": S, "subints_asked": S_asked, "total_ops": total_ops,
+        "plane_bytes": plane_bytes,
         "plain_ms": t_plain, "plain_tops": total_ops / t_plain / 1e9,
         "plain_launches_per_pass": S * len(probs),
         "graph_ms": t_graph, "graph_tops": total_ops / t_graph / 1e9,
