@@ -892,7 +892,7 @@ def cpu_leg(line, hp_sub, checks, batched_samples, args):
     out = {}
     if hp_sub is not None and not args.no_cpu_baseline:
         configure(None, "plain")
-        gbps, cores, desc, _, ref = cpu_correlator_sample(oracle, hp_sub, target_s=args.cpu_seconds)
+        gbps, cores, desc, _, _ = cpu_correlator_sample(oracle, hp_sub, target_s=args.cpu_seconds)
         line["cpu_baseline"] = {"value": gbps, "unit": "Gb/s", "cores": cores, "kind": "port",
                                 "sample": desc}
     for name, ck in checks:
