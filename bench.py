@@ -491,7 +491,7 @@ def vis_checksum(torch, v):
 
 
 def batched_block(torch, mixer, dev, S=4, small=False, rounds=5, reps=2, tune_reps=1,
-                  check_arrays=3):
+                  check_arrays=3, n_arrays=48):
     """48 uneven arrays, S sub-integrations of each per pass.  Plain form: one
     GEMM launch per array and sub-integration (K samples each, int64 added per
     launch), the reference's per-V-update launch form.  Batched form: ONE
@@ -502,7 +502,7 @@ def batched_block(torch, mixer, dev, S=4, small=False, rounds=5, reps=2, tune_re
     forms read the same bytes.  Results: plain == batched per array (checksum),
     and the sampled arrays' V go to the CPU leg for the oracle check."""
     stream = torch.cuda.Stream()
-    arrays = batched_arrays(small=small)
+    arrays = batched_arrays(small=small)[:n_arrays]
     # the largest S up to the one asked for whose planes, cubes and packet buffer fit
     # in 90 % of the free device memory
     free, _ = torch.cuda.mem_get_info(dev)
@@ -598,8 +598,9 @@ def batched_block(torch, mixer, dev, S=4, small=False, rounds=5, reps=2, tune_re
                         "got": unpack_channels(torch, mixer, p["vis"], n, chans)})
     exact_vs_plain = sums_plain == sums_batch and info["kernel_err"] == 0
     out = {
-        "workload": ("48 small arrays, N in {64..256 step 32}, C in {16..64 step 16}" if small else
-                     "48 arrays, N in {64..1024 step 32}, C in {16..512 step 16}")
+        "workload": (f"{len(arrays)} of 48 " if len(arrays) < 48 else "48 ")
+        + ("small arrays, N in {64..256 step 32}, C in {16..64 step 16}" if small else
+           "arrays, N in {64..1024 step 32}, C in {16..512 step 16}")
         + f", K in {{256..4096 step 256}} per sub-integration, {S} sub-integrations per pass, "
           "1 source + sigma 12 noise each (seeded)",
         "subints_per_pass": S, "subints_asked": S_asked, "total_ops": total_ops,
@@ -1242,7 +1243,7 @@ def run_batched(args):
     dev = torch.device("cuda:0")
     torch.cuda.set_device(dev)
     out, samples = batched_block(torch, mixer, dev, S=args.batched_subints, small=args.small_arrays,
-                                 rounds=5, reps=3, tune_reps=args.tune_reps)
+                                 rounds=5, reps=3, tune_reps=args.tune_reps, n_arrays=args.arrays)
     line = {"metric": "batched uneven arrays: int8 cGEMM TOPS (triangle basis), batched vs plain",
             "batched": out}
     if not args.no_cpu_baseline:
@@ -1564,6 +1565,8 @@ def main():
                     help="only the 1024-element workload (no small / large / batched / serve)")
     ap.add_argument("--batched-subints", type=int, default=4,
                     help="sub-integrations per array per batched pass")
+    ap.add_argument("--arrays", type=int, default=48,
+                    help="--config batched: the first N arrays of the seeded draw (small ncu cases)")
     ap.add_argument("--tune-reps", type=int, default=1,
                     help="launches per autotuner sample (0: no autotuning, the default plan)")
     ap.add_argument("--nch", type=int, default=0,
