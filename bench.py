@@ -463,7 +463,23 @@ def workload_summary(r, probe=None):
         kind = "sustained" if r["ms_total"] > SUSTAINED_REGION_MS else "burst"
         out["gemm_frac_of_int8_peak"] = tops / probe[kind]["tops"]
         out["int8_peak_kind"] = kind
+        # the GEMM's own roofline: its algorithmic bytes per launch (planes read once,
+        # int64 cube read and written) against its ops; the bound is the lower of the
+        # measured int8 rate and intensity x HBM bandwidth
+        gbytes = 2 * NCH * NANT * r["kt"] + 2 * 8 * mixer_vis_elems_host(NANT, NCH)
+        ai = tri_ops(r["kt"]) / gbytes
+        mem_tops = ai * hbm / 1e3
+        peak = min(probe[kind]["tops"], mem_tops)
+        out["gemm_roofline"] = {"ops_per_byte": ai, "bound": "hbm" if mem_tops < probe[kind]["tops"]
+                                else "tensor", "peak_tops": peak, "frac": tops / peak,
+                                "basis": "triangle ops over planes + int64 cube RMW bytes"}
     return out
+
+
+def mixer_vis_elems_host(nant, nch):
+    """Tile-packed cube elements (re + im), as mixer_vis_elems computes them."""
+    nb = (nant + 127) // 128
+    return nch * nb * (nb + 1) // 2 * 2 * 128 * 128
 
 
 # ---------------------------------------------------------------- batched ----
