@@ -47,6 +47,8 @@ struct mixer_batch {
     int32_t order;
     int32_t grid;
     int32_t* d_err;
+    unsigned long long* d_ctr;   // item counter of the launch
+    bool ragged;                 // some array's N is not a multiple of 128
     cudaGraph_t graph;
     cudaGraphExec_t exec;
 };
@@ -79,6 +81,9 @@ static int build_work(mixer_batch* b, std::vector<mixer::XcorrWork>& w) {
                     w.push_back(it);
                 }
     }
+    // Longest first by K extent; the stable sort keeps each channel's tiles
+    // (ragged-block tiles included) next to each other, so the CTAs that
+    // share a channel's row blocks run together and read them from L2.
     if (b->order == MIXER_ORDER_LPT)
         std::stable_sort(w.begin(), w.end(), [](const mixer::XcorrWork& a, const mixer::XcorrWork& c) {
             return a.nkc > c.nkc;
@@ -121,6 +126,7 @@ extern "C" int mixer_batch_destroy(mixer_batch* b) {
     cudaFree(b->d_probs);
     cudaFree(b->d_work);
     cudaFree(b->d_err);
+    cudaFree(b->d_ctr);
     delete b;
     return MIXER_OK;
 }
@@ -145,7 +151,7 @@ extern "C" int mixer_batch_create(const mixer_xcorr_problem* probs, int32_t npro
     b->order = MIXER_ORDER_LPT;
     b->probs.assign(probs, probs + nprob);
     int rc = MIXER_OK;
-    std::vector<CUtensorMap> maps(nprob);
+    std::vector<CUtensorMap> maps(2 * (size_t)nprob);   // two per problem
     b->tprobs.resize(nprob);
     // problems whose cubes overlap share tiles: their items always add atomically
     b->shared_cube.assign(nprob, 0);
@@ -163,8 +169,9 @@ extern "C" int mixer_batch_create(const mixer_xcorr_problem* probs, int32_t npro
     }
     for (int p = 0; p < nprob && rc == MIXER_OK; ++p) {
         const mixer_xcorr_problem& q = probs[p];
-        rc = mixer::xcorr_encode_map(&maps[p], q.planes, q.nant, q.nch, q.kt, q.kbeg + q.klen);
+        rc = mixer::xcorr_encode_maps(&maps[2 * p], q.planes, q.nant, q.nch, q.kt, q.kbeg + q.klen);
         const int nb = nblk_of(q.nant);
+        if (q.nant % 128) b->ragged = true;
         b->tprobs[p] = mixer::XcorrProblem{q.nant, q.nch, nb * (nb + 1) / 2, (int32_t)q.kbeg, q.mode, 0,
                                            q.vis};
     }
@@ -175,11 +182,12 @@ extern "C" int mixer_batch_create(const mixer_xcorr_problem* probs, int32_t npro
     if (rc != MIXER_OK) return fail(rc);
     cudaError_t e;
     if ((e = cudaGetDevice(&b->dev)) != cudaSuccess) return fail(mixer::cuda_status(e, "cudaGetDevice"));
-    if ((e = cudaMalloc(&b->d_maps, nprob * sizeof(CUtensorMap))) != cudaSuccess ||
+    if ((e = cudaMalloc(&b->d_maps, maps.size() * sizeof(CUtensorMap))) != cudaSuccess ||
         (e = cudaMalloc(&b->d_probs, nprob * sizeof(mixer::XcorrProblem))) != cudaSuccess ||
         (e = cudaMalloc(&b->d_err, sizeof(int32_t))) != cudaSuccess ||
-        (e = cudaMemcpy(b->d_maps, maps.data(), nprob * sizeof(CUtensorMap), cudaMemcpyHostToDevice)) !=
-            cudaSuccess ||
+        (e = cudaMalloc(&b->d_ctr, sizeof(unsigned long long))) != cudaSuccess ||
+        (e = cudaMemcpy(b->d_maps, maps.data(), maps.size() * sizeof(CUtensorMap),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(b->d_probs, b->tprobs.data(), nprob * sizeof(mixer::XcorrProblem),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemset(b->d_err, 0, sizeof(int32_t))) != cudaSuccess)
@@ -205,6 +213,7 @@ extern "C" int mixer_batch_plan(mixer_batch* b, const int32_t* split_per_class, 
 extern "C" int mixer_batch_run(mixer_batch* b, void* stream) {
     if (!b) return MIXER_EINVAL;
     return mixer::xcorr_launch_table(b->d_maps, b->d_probs, b->d_work, b->nwork, b->grid, b->d_err,
+                                     b->d_ctr, b->ragged,
                                      static_cast<cudaStream_t>(stream));
 }
 

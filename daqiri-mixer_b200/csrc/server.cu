@@ -168,6 +168,7 @@ struct mixer_server {
     bool table_used[2] = {false, false};
     int tsel = 0;
     int32_t* d_err = nullptr;
+    unsigned long long* d_ctr = nullptr;   // item counter of the GEMM launches (stream comp)
     // Stream state comes from a server-owned stream-ordered pool and pinned dump
     // buffers are recycled, so opening or closing a stream never runs the
     // device-wide synchronisation of cudaMalloc / cudaFree / cudaFreeHost while
@@ -265,8 +266,10 @@ bool serve_once(mixer_server* sv) {
     std::vector<CUtensorMap> maps;
     std::vector<mixer::XcorrProblem> probs;
     std::vector<mixer::XcorrWork> work;
+    bool ragged = false;
     for (size_t r = 0; r < ready.size(); ++r) {
         Stream& s = sv->streams[ready[r].sid];
+        if (s.d.nant % 128) ragged = true;
         // corner-turn the ready sub-integrations, one launch per contiguous run of ring slots
         for (int64_t q = 0; q < ready[r].nsub;) {
             const int64_t sub = ready[r].sub0 + q;
@@ -287,10 +290,11 @@ bool serve_once(mixer_server* sv) {
         const int ntiles = nb * (nb + 1) / 2;
         const int64_t klen = ready[r].nsub * s.d.ksub;
         const uint32_t nkc = (uint32_t)((klen + 127) / 128);
-        CUtensorMap m;
-        const int mrc = mixer::xcorr_encode_map(&m, s.planes, s.d.nant, s.d.nch, s.kt, klen);
+        CUtensorMap m[2];
+        const int mrc = mixer::xcorr_encode_maps(m, s.planes, s.d.nant, s.d.nch, s.kt, klen);
         if (mrc != MIXER_OK) sv->error.store(mrc);
-        maps.push_back(m);
+        maps.push_back(m[0]);
+        maps.push_back(m[1]);
         // one item per (channel, tile) over all ready sub-integrations, and every
         // stream has a cube of its own: the items own their tiles
         probs.push_back(mixer::XcorrProblem{s.d.nant, s.d.nch, ntiles, 0, MIXER_VIS_ACC_I64, 1, s.vis});
@@ -332,18 +336,18 @@ bool serve_once(mixer_server* sv) {
         sv->work_cap[ts] = (int64_t)cap;
     }
     if (sv->error.load()) return false;
-    memcpy(sv->h_maps[ts], maps.data(), np * sizeof(CUtensorMap));
+    memcpy(sv->h_maps[ts], maps.data(), maps.size() * sizeof(CUtensorMap));
     memcpy(sv->h_probs[ts], probs.data(), np * sizeof(mixer::XcorrProblem));
     memcpy(sv->h_work[ts], work.data(), work.size() * sizeof(mixer::XcorrWork));
-    cudaMemcpyAsync(sv->d_maps[ts], sv->h_maps[ts], np * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
-                    comp);
+    cudaMemcpyAsync(sv->d_maps[ts], sv->h_maps[ts], maps.size() * sizeof(CUtensorMap),
+                    cudaMemcpyHostToDevice, comp);
     cudaMemcpyAsync(sv->d_probs[ts], sv->h_probs[ts], np * sizeof(mixer::XcorrProblem),
                     cudaMemcpyHostToDevice, comp);
     cudaMemcpyAsync(sv->d_work[ts], sv->h_work[ts], work.size() * sizeof(mixer::XcorrWork),
                     cudaMemcpyHostToDevice, comp);
     const int rc = mixer::xcorr_launch_table(sv->d_maps[ts], sv->d_probs[ts], sv->d_work[ts],
                                              (int64_t)work.size(), mixer::xcorr_sm_count(), sv->d_err,
-                                             comp);
+                                             sv->d_ctr, ragged, comp);
     if (rc != MIXER_OK) sv->error.store(rc);
     cudaEventRecord(sv->table_free[ts], comp);
     sv->table_used[ts] = true;
@@ -527,15 +531,17 @@ extern "C" int mixer_server_create(const mixer_server_cfg* cfg, mixer_server** o
         }
     }
     for (int t = 0; t < 2; ++t) {
-        if ((e = cudaMalloc(&sv->d_maps[t], cfg->max_streams * sizeof(CUtensorMap))) != cudaSuccess ||
+        // two tensor maps per stream (xcorr_encode_maps)
+        if ((e = cudaMalloc(&sv->d_maps[t], 2 * cfg->max_streams * sizeof(CUtensorMap))) != cudaSuccess ||
             (e = cudaMalloc(&sv->d_probs[t], cfg->max_streams * sizeof(mixer::XcorrProblem))) != cudaSuccess ||
-            (e = cudaMallocHost(&sv->h_maps[t], cfg->max_streams * sizeof(CUtensorMap))) != cudaSuccess ||
+            (e = cudaMallocHost(&sv->h_maps[t], 2 * cfg->max_streams * sizeof(CUtensorMap))) != cudaSuccess ||
             (e = cudaMallocHost(&sv->h_probs[t], cfg->max_streams * sizeof(mixer::XcorrProblem))) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&sv->table_free[t], cudaEventDisableTiming)) != cudaSuccess)
             return fail(e, "server tables");
     }
     if ((e = cudaMalloc(&sv->d_err, sizeof(int32_t))) != cudaSuccess ||
-        (e = cudaMemset(sv->d_err, 0, sizeof(int32_t))) != cudaSuccess)
+        (e = cudaMemset(sv->d_err, 0, sizeof(int32_t))) != cudaSuccess ||
+        (e = cudaMalloc(&sv->d_ctr, sizeof(unsigned long long))) != cudaSuccess)
         return fail(e, "server error word");
     sv->worker = std::thread(worker_main, sv);
     *out = sv;
@@ -569,6 +575,7 @@ extern "C" int mixer_server_destroy(mixer_server* sv) {
         if (sv->table_free[t]) cudaEventDestroy(sv->table_free[t]);
     }
     cudaFree(sv->d_err);
+    cudaFree(sv->d_ctr);
     if (sv->copy) cudaStreamDestroy(sv->copy);
     if (sv->comp) cudaStreamDestroy(sv->comp);
     if (sv->d2h) cudaStreamDestroy(sv->d2h);

@@ -15,8 +15,14 @@
 //
 // No operand is ever negated, so every int8 input, -128 included, is exact.
 // Diagonal tiles (i == j) use the A tiles [Xr_i ; Xi_i] as B and load half
-// the bytes.  Operands come from the corner-turned planes [2][C][N][kt]
-// through 4-D TMA tensor loads (128-byte swizzle, 128 x 128-byte boxes)
+// the bytes.  When N is not a multiple of 128 the last block holds r < 128
+// antennas; its tiles put that block on the N side with r16 = r rounded up to
+// 16 rows per plane (N = 2 r16): tile (nb-1, j < nb-1) is computed as its
+// conjugate transpose, A = block j and B = [Xr_nb-1 ; Xi_nb-1] (r16 rows
+// each, one TMA box over both planes), and written back transposed; tile
+// (nb-1, nb-1) keeps A = its own block.  Operands come from the corner-turned
+// planes [2][C][N][kt] through 4-D TMA tensor loads (128-byte swizzle,
+// 128 x 128-byte boxes)
 // into a 3-deep shared-memory ring.  One elected thread issues all
 // tcgen05.mma; the int32 accumulators stay in TMEM for the whole K range of
 // the launch; eight epilogue warps read them back with tcgen05.ld and add
@@ -24,10 +30,15 @@
 //
 // Warp roles (320 threads with the default build, one CTA per SM, persistent
 // over work items):
-//   warp 0      TMA producer
+//   warp 0      TMA producer; picks the CTA's next item and passes its index
+//               to the other roles through a shared-memory ring
 //   warp 1      TMEM allocator + MMA issuer
 //   warps 2..9  epilogue (TMEM lane quadrant = warp % 4, 64-column half =
 //               (warp - 2) / 4)
+// A single-array launch hands CTA b the items b, b + grid, ... (all items
+// but the ragged block's cost the same); a table launch takes items in list
+// order from a global counter, so CTAs stay on neighbouring items, which
+// share operand blocks in L2, whatever each item costs.
 #include "common.cuh"
 #include "xcorr.cuh"
 #include <cstdlib>
@@ -65,6 +76,17 @@ namespace {
 #ifndef MIXER_XCORR_DIAG3
 #define MIXER_XCORR_DIAG3 0
 #endif
+// Tiles of a ragged last block (N not a multiple of 128) with the block on the
+// MMA's N side, N = 2 r16 (1), or as full 128 x 128 tiles with zero rows (0).
+#ifndef MIXER_XCORR_TAIL
+#define MIXER_XCORR_TAIL 1
+#endif
+// Transposed ragged tiles: each warp passes its 32 x 16 blocks through shared
+// memory so that a warp's adds cover two 128-byte lines per instruction (1),
+// or adds straight from the TMEM rows, 32 lines per instruction (0).
+#ifndef MIXER_XCORR_TAIL_XPOSE
+#define MIXER_XCORR_TAIL_XPOSE 1
+#endif
 constexpr int kTile = 128;                       // tile rows = cols
 constexpr int kWorkChunk = 128;                  // samples per work-list K unit
 constexpr int kKc = MIXER_XCORR_KC;              // samples (bytes) per pipeline stage
@@ -77,7 +99,14 @@ constexpr int kEpiGroups = MIXER_XCORR_EPI_GROUPS;  // column groups per TMEM la
 constexpr int kEpiWarps = 4 * kEpiGroups;
 constexpr int kEpiCols = kTile / kEpiGroups;     // 64 columns per warp
 constexpr int kThreads = 64 + 32 * kEpiWarps;
-constexpr int kBarBytes = 256;
+constexpr int kBarBytes = 512;
+// Item ring (table launches take items from a global counter): the producer
+// publishes each item index to the MMA and epilogue warps through kItemSlots
+// slots after the pipeline barriers.
+constexpr int kItemSlots = 8;
+constexpr int kItemBar0 = 24;                    // first ring barrier (uint64 index)
+static_assert(2 * MIXER_XCORR_STAGES + 5 <= kItemBar0, "barrier area");
+static_assert((kItemBar0 + 3 * kItemSlots) * 8 <= kBarBytes, "barrier area");
 // The diagonal-tile exchange needs the 2 x 4 layout of eight epilogue warps.
 constexpr bool kDiag3 = MIXER_XCORR_DIAG3 != 0 && kEpiGroups == 2;
 // Exchange area: one round's eight 32 x 32 int32 blocks of P2, rows padded to
@@ -86,7 +115,15 @@ constexpr bool kDiag3 = MIXER_XCORR_DIAG3 != 0 && kEpiGroups == 2;
 constexpr int kXchgStride = 33;
 constexpr int kXchgBlock = 32 * kXchgStride;     // words per block
 constexpr int kXchgBytes = kDiag3 ? 8 * kXchgBlock * 4 : 0;
-constexpr int kSmemBytes = kStages * kStageBytes + 1024 + kBarBytes + kXchgBytes;
+// Transpose area of the ragged tiles: per epilogue warp 32 rows of 16 words,
+// padded to 17 (row writes and the two-rows-per-read pattern are conflict-free).
+// It shares the exchange area (the two serve different items).
+constexpr int kXposeStride = 17;
+constexpr int kXposeBytes =
+    (MIXER_XCORR_TAIL && MIXER_XCORR_TAIL_XPOSE) ? kEpiWarps * 32 * kXposeStride * 4 : 0;
+constexpr int kEpiSmemBytes = kXchgBytes > kXposeBytes ? kXchgBytes : kXposeBytes;
+constexpr int kSmemBase = kStages * kStageBytes + 1024 + kBarBytes;
+constexpr int kSmemBytes = kSmemBase + kEpiSmemBytes;   // the most a launch asks for
 static_assert(kSmemBytes <= 232448, "shared memory");
 constexpr uint32_t kTmemCols = 512;              // D1 (256) + D2 (256)
 constexpr uint32_t kIdesc = idesc_i8(128, 256);
@@ -101,7 +138,12 @@ struct XcorrArgs {
     int64_t nwork;       // nch * ntiles, or the length of `work`
     void* vis;
     int32_t* err;
+    // Item counter of a table launch, zero at its start (nullptr: CTA b takes
+    // items b, b + grid, ...).
+    unsigned long long* ctr;
     // Batched mode (work != nullptr): per-array tensor maps, problems, work list.
+    // Two maps per array: [2p] the 128-row operand boxes, [2p + 1] the ragged
+    // last block's box over both planes.
     const CUtensorMap* tmaps;
     const XcorrProblem* probs;
     const XcorrWork* work;
@@ -121,16 +163,28 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
 
 struct Item {
     const CUtensorMap* map;
+    const CUtensorMap* map_tail;
     void* vis;
     int c, t, i, j, kbeg, kc0, nkc, mode, ntiles, excl;
+    int tail;   // rows per plane of the ragged last block on the N side (0: full tile)
 };
 
-__device__ __forceinline__ Item get_item(const XcorrArgs& a, const CUtensorMap* pmap, int64_t w) {
+// Rows per plane of the last 128-row block rounded up to 16 (128 when full).
+__host__ __device__ __forceinline__ int tail_rows(int nant) {
+    const int r = nant - ((nant - 1) / kTile) * kTile;
+    return (r + 15) & ~15;
+}
+
+__device__ __forceinline__ Item get_item(const XcorrArgs& a, const CUtensorMap* pmap,
+                                         const CUtensorMap* pmap_tail, int64_t w) {
     Item it;
+    int nant;
     if (a.work == nullptr) {
         it.c = (int)(w / a.ntiles);
         it.t = (int)(w - (int64_t)it.c * a.ntiles);
         it.map = pmap;
+        it.map_tail = pmap_tail;
+        nant = a.nant;
         it.vis = a.vis;
         it.kbeg = a.kbeg;
         it.kc0 = 0;
@@ -143,7 +197,9 @@ __device__ __forceinline__ Item get_item(const XcorrArgs& a, const CUtensorMap* 
         const XcorrProblem& pr = a.probs[wk.prob];
         it.c = (int)wk.chan;
         it.t = (int)wk.tile;
-        it.map = a.tmaps + wk.prob;
+        it.map = a.tmaps + 2 * wk.prob;
+        it.map_tail = it.map + 1;
+        nant = pr.nant;
         it.vis = pr.vis;
         it.kbeg = pr.kbeg;
         it.kc0 = (int)wk.kc0;
@@ -153,6 +209,8 @@ __device__ __forceinline__ Item get_item(const XcorrArgs& a, const CUtensorMap* 
         it.excl = pr.excl;
     }
     decode_tile(it.t, it.i, it.j);
+    const int r16 = tail_rows(nant);
+    it.tail = (MIXER_XCORR_TAIL && r16 < kTile && it.i == (nant - 1) / kTile) ? r16 : 0;
     return it;
 }
 
@@ -204,8 +262,11 @@ __device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-// Adds (or stores) 16 columns of one row of a tile into the cube: element e at
-// e0 + e * 128 of the re plane and the im plane kTile * kTile further on.
+// Adds (or stores) 16 elements of one row of TMEM into the cube: element e at
+// e0 + e * kStride of the re plane and the im plane kTile * kTile further on
+// (kStride 128: 16 columns of a tile row; 1: 16 rows of a tile column, for a
+// tile computed as its conjugate transpose).
+template <int kStride>
 __device__ __forceinline__ void store16(const Item& it, size_t e0, const int32_t (&re)[16],
                                         const int32_t (&im)[16]) {
     if (it.mode == MIXER_VIS_ACC_I64 && MIXER_XCORR_EXCL_RMW && it.excl) {
@@ -215,40 +276,55 @@ __device__ __forceinline__ void store16(const Item& it, size_t e0, const int32_t
         long long a[16], b[16];
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
-            a[e] = v[e * kTile];
-            b[e] = v[e * kTile + kTile * kTile];
+            a[e] = v[e * kStride];
+            b[e] = v[e * kStride + kTile * kTile];
         }
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
-            v[e * kTile] = a[e] + (long long)re[e];
-            v[e * kTile + kTile * kTile] = b[e] + (long long)im[e];
+            v[e * kStride] = a[e] + (long long)re[e];
+            v[e * kStride + kTile * kTile] = b[e] + (long long)im[e];
         }
     } else if (it.mode == MIXER_VIS_ACC_I64) {
         unsigned long long* v = reinterpret_cast<unsigned long long*>(it.vis) + e0;
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
-            atomicAdd(v + e * kTile, (unsigned long long)(long long)re[e]);
-            atomicAdd(v + e * kTile + kTile * kTile, (unsigned long long)(long long)im[e]);
+            atomicAdd(v + e * kStride, (unsigned long long)(long long)re[e]);
+            atomicAdd(v + e * kStride + kTile * kTile, (unsigned long long)(long long)im[e]);
         }
     } else if (it.mode == MIXER_VIS_ACC_I32) {
         int* v = reinterpret_cast<int*>(it.vis) + e0;
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
-            atomicAdd(v + e * kTile, re[e]);
-            atomicAdd(v + e * kTile + kTile * kTile, im[e]);
+            atomicAdd(v + e * kStride, re[e]);
+            atomicAdd(v + e * kStride + kTile * kTile, im[e]);
         }
     } else {
         int* v = reinterpret_cast<int*>(it.vis) + e0;
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
-            v[e * kTile] = re[e];
-            v[e * kTile + kTile * kTile] = im[e];
+            v[e * kStride] = re[e];
+            v[e * kStride + kTile * kTile] = im[e];
         }
     }
 }
 
+// Adds (or stores) one element of the cube, in the item's mode.
+__device__ __forceinline__ void store1(const Item& it, size_t e, int32_t x) {
+    if (it.mode == MIXER_VIS_ACC_I64 && MIXER_XCORR_EXCL_RMW && it.excl) {
+        long long* v = reinterpret_cast<long long*>(it.vis) + e;
+        *v += (long long)x;
+    } else if (it.mode == MIXER_VIS_ACC_I64) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(it.vis) + e, (unsigned long long)(long long)x);
+    } else if (it.mode == MIXER_VIS_ACC_I32) {
+        atomicAdd(reinterpret_cast<int*>(it.vis) + e, x);
+    } else {
+        reinterpret_cast<int*>(it.vis)[e] = x;
+    }
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
-    k_xcorr_tri(const __grid_constant__ CUtensorMap tmap, const XcorrArgs args) {
+    k_xcorr_tri(const __grid_constant__ CUtensorMap tmap,
+                const __grid_constant__ CUtensorMap tmap_tail, const XcorrArgs args) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;           // 1 KiB aligned (swizzle atoms)
@@ -257,11 +333,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 4);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     int32_t* xchg = reinterpret_cast<int32_t*>(gbase + kStages * kStageBytes + kBarBytes);
+    volatile int64_t* witems = reinterpret_cast<volatile int64_t*>(bars + kItemBar0 + 2 * kItemSlots);
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int FULL = 0, EMPTY = kStages, ACCF = 2 * kStages, ACCE = 2 * kStages + 1,
-              DRAIN = 2 * kStages + 2;
+              DRAIN = 2 * kStages + 2, IFULL = kItemBar0, IEMPTY = kItemBar0 + kItemSlots;
     auto bar = [&](int k) { return smem_u32(&bars[k]); };
 
     if (threadIdx.x == 0) {
@@ -272,10 +349,17 @@ __global__ void __launch_bounds__(kThreads, 1)
         mbar_init(bar(ACCF), 1);
         mbar_init(bar(ACCE), 32 * kEpiWarps);
         mbar_init(bar(DRAIN), 1);
+        for (int s = 0; s < kItemSlots; ++s) {
+            mbar_init(bar(IFULL + s), 1);
+            mbar_init(bar(IEMPTY + s), 1 + kEpiWarps);   // the MMA thread, one per epilogue warp
+        }
         *abort_flag = 0;
         fence_mbar_init();
     }
-    if (warp == 0 && lane == 0 && args.work == nullptr) prefetch_tmap(&tmap);
+    if (warp == 0 && lane == 0 && args.work == nullptr) {
+        prefetch_tmap(&tmap);
+        prefetch_tmap(&tmap_tail);
+    }
     if (warp == 1) {
         tmem_alloc(smem_u32(tmem_slot), kTmemCols);
         tmem_relinquish();
@@ -292,10 +376,29 @@ __global__ void __launch_bounds__(kThreads, 1)
             uint32_t phase = 0;
             int64_t issued = 0;
             bool ok = true;
-            for (int64_t w = blockIdx.x; w < args.nwork && ok; w += gridDim.x) {
-                const Item it = get_item(args, &tmap, w);
+            int islot = 0;
+            uint32_t iphase = 0;
+            int64_t w = blockIdx.x;
+            while (ok) {
+                // publish the item (or the end mark -1) to the MMA and epilogue warps
+                if (w >= args.nwork) w = -1;
+                if (!mbar_wait(bar(IEMPTY + islot), iphase ^ 1u, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                witems[islot] = w;
+                mbar_arrive(bar(IFULL + islot));
+                if (++islot == kItemSlots) {
+                    islot = 0;
+                    iphase ^= 1u;
+                }
+                if (w < 0) break;
+                const Item it = get_item(args, &tmap, &tmap_tail, w);
                 const bool diag = (it.i == it.j);
-                const uint32_t bytes = diag ? 2 * kTileBytes : 4 * kTileBytes;
+                const uint32_t bytes = it.tail ? 2 * kTileBytes + 2 * it.tail * kKc
+                                               : (diag ? 2 * kTileBytes : 4 * kTileBytes);
+                // A block: block j for a transposed ragged tile, else block i
+                const int ia = (it.tail && !diag) ? it.j : it.i;
                 for (int kc = 0; kc < it.nkc * kSubPerChunk; ++kc) {
                     if (!mbar_wait(bar(EMPTY + stage), phase ^ 1u, abort_flag)) {
                         ok = false;
@@ -305,9 +408,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const uint32_t fb = bar(FULL + stage);
                     mbar_expect_tx(fb, bytes);
                     const int k = it.kbeg + it.kc0 * kWorkChunk + kc * kKc;
-                    tma_load_4d(sb + 0 * kTileBytes, it.map, fb, k, it.i * kTile, it.c, 0);
-                    tma_load_4d(sb + 1 * kTileBytes, it.map, fb, k, it.i * kTile, it.c, 1);
-                    if (!diag) {
+                    tma_load_4d(sb + 0 * kTileBytes, it.map, fb, k, ia * kTile, it.c, 0);
+                    tma_load_4d(sb + 1 * kTileBytes, it.map, fb, k, ia * kTile, it.c, 1);
+                    if (it.tail) {
+                        // [Xr ; Xi] of the ragged block, it.tail rows each, one box
+                        tma_load_4d(sb + 2 * kTileBytes, it.map_tail, fb, k, it.i * kTile, it.c, 0);
+                    } else if (!diag) {
                         tma_load_4d(sb + 2 * kTileBytes, it.map, fb, k, it.j * kTile, it.c, 0);
                         tma_load_4d(sb + 3 * kTileBytes, it.map, fb, k, it.j * kTile, it.c, 1);
                     }
@@ -317,6 +423,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                         phase ^= 1u;
                     }
                 }
+                // next item: in list order from the launch's counter, or round robin
+                w = args.ctr ? (int64_t)gridDim.x + (int64_t)atomicAdd(args.ctr, 1ull)
+                             : w + gridDim.x;
             }
             if (!ok) {
                 if (args.err) atomicOr(args.err, 1);
@@ -333,9 +442,23 @@ __global__ void __launch_bounds__(kThreads, 1)
             uint32_t phase = 0, acc_phase = 0;
             bool ok = true;
             const uint32_t t_d1 = tmem, t_d2 = tmem + 256;
-            for (int64_t w = blockIdx.x; w < args.nwork; w += gridDim.x) {
-                const Item it = get_item(args, &tmap, w);
+            int islot = 0;
+            uint32_t iphase = 0;
+            while (true) {
+                if (!mbar_wait(bar(IFULL + islot), iphase, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                const int64_t w = witems[islot];
+                mbar_arrive(bar(IEMPTY + islot));
+                if (++islot == kItemSlots) {
+                    islot = 0;
+                    iphase ^= 1u;
+                }
+                if (w < 0) break;
+                const Item it = get_item(args, &tmap, &tmap_tail, w);
                 const bool diag = (it.i == it.j);
+                const uint32_t id1 = it.tail ? idesc_i8(128, 2 * it.tail) : kIdesc;
                 if (!mbar_wait(bar(ACCE), acc_phase ^ 1u, abort_flag)) {
                     ok = false;
                     break;
@@ -350,17 +473,18 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const uint32_t sb = base + stage * kStageBytes;
                     const uint64_t ar = sdesc(sb);
                     const uint64_t ai = sdesc(sb + kTileBytes);
-                    // 256-row B operand [Xr_j ; Xi_j]: two adjacent tiles
-                    const uint64_t b = diag ? ar : sdesc(sb + 2 * kTileBytes);
+                    // 256-row B operand [Xr_j ; Xi_j]: two adjacent tiles (2 it.tail
+                    // rows for a ragged block)
+                    const uint64_t b = (diag && !it.tail) ? ar : sdesc(sb + 2 * kTileBytes);
                     // diagonal tiles: D2 = Xi Xi^T (N 128) instead of Xi [Xr ; Xi]^T
-                    const bool three = kDiag3 && diag;
+                    const bool three = kDiag3 && diag && !it.tail;
                     const uint64_t b2 = three ? ai : b;
-                    const uint32_t id2 = three ? kIdescN128 : kIdesc;
+                    const uint32_t id2 = three ? kIdescN128 : id1;
 #pragma unroll
                     for (int kk = 0; kk < kKc / 32; ++kk) {
                         const uint64_t o = (uint64_t)((kk * 32) >> 4);   // 32-byte K step
                         const uint32_t acc = (kc > 0 || kk > 0) ? 1u : 0u;
-                        mma_i8(t_d1, ar + o, b + o, kIdesc, acc);
+                        mma_i8(t_d1, ar + o, b + o, id1, acc);
                         mma_i8(t_d2, ai + o, b2 + o, id2, acc);
                     }
                     tc_commit(bar(EMPTY + stage));   // stage free once these MMAs finish
@@ -391,8 +515,23 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int m = q * 32 + lane;
         const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)col0;
         uint32_t acc_phase = 0;
-        for (int64_t w = blockIdx.x; w < args.nwork; w += gridDim.x) {
-            const Item it = get_item(args, &tmap, w);
+        int islot = 0;
+        uint32_t iphase = 0;
+        while (true) {
+            if (!mbar_wait(bar(IFULL + islot), iphase, abort_flag)) {
+                if (args.err) atomicOr(args.err, 4);
+                *abort_flag = 1;
+                break;
+            }
+            const int64_t w = witems[islot];
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar(IEMPTY + islot));
+            if (++islot == kItemSlots) {
+                islot = 0;
+                iphase ^= 1u;
+            }
+            if (w < 0) break;
+            const Item it = get_item(args, &tmap, &tmap_tail, w);
             if (!mbar_wait(bar(ACCF), acc_phase, abort_flag)) {
                 if (args.err) atomicOr(args.err, 4);
                 *abort_flag = 1;
@@ -400,7 +539,81 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             tc_fence_after();
             const size_t tb = ((size_t)it.c * it.ntiles + it.t) * (size_t)(2 * kTile * kTile);
-            if (!(kDiag3 && it.i == it.j)) {
+            if (it.tail) {
+                // Ragged last block on the N side: columns n < it.tail of each
+                // product (R1 | P2 at 0 | it.tail, P1 | R2 at 256 | 256 + it.tail).
+                // Transposed tile (i != j): TMEM row m is column m of tile (i, j)
+                // and column n its row n, so Re = R1 + R2, Im = P2 - P1 and the
+                // 16 values of a load belong to 16 consecutive rows.  Chunks of
+                // 16 columns alternate between the column groups; in store mode
+                // the rows past it.tail are written as zeros.
+                const bool tr = it.i != it.j;
+                const int g = (warp - 2) >> 2;
+                const int nt = it.tail;
+                const int ncols = it.mode == MIXER_VIS_STORE_I32 ? kTile : nt;
+                const uint32_t tq = tmem + ((uint32_t)(q * 32) << 16);
+                int last = -1;   // this warp's last chunk that reads TMEM
+                for (int n0 = 16 * g; n0 < nt; n0 += 16 * kEpiGroups) last = n0;
+                if (last < 0) {
+                    tc_fence_before();
+                    mbar_arrive(bar(ACCE));
+                }
+#pragma unroll 1
+                for (int n0 = 16 * g; n0 < ncols; n0 += 16 * kEpiGroups) {
+                    int32_t re[16], im[16];
+                    if (n0 < nt) {
+                        uint32_t r[4][16];   // R1, P2, P1, R2
+                        tmem_ld4_x16(tq + n0, tq + nt + n0, tq + 256 + n0, tq + 256 + nt + n0, r);
+                        if (n0 == last) {
+                            tc_fence_before();
+                            mbar_arrive(bar(ACCE));
+                        }
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) {
+                            re[e] = (int32_t)(r[0][e] + r[3][e]);
+                            im[e] = tr ? (int32_t)(r[1][e] - r[2][e]) : (int32_t)(r[2][e] - r[1][e]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) re[e] = im[e] = 0;
+                    }
+                    if (tr && it.mode == MIXER_VIS_STORE_I32 &&
+                        (reinterpret_cast<uintptr_t>(it.vis) & 15) == 0) {
+                        // stores: a thread's 16 elements are contiguous, 4 x 16 bytes
+                        int4* vr = reinterpret_cast<int4*>(reinterpret_cast<int*>(it.vis) + tb +
+                                                           (size_t)m * kTile + n0);
+                        int4* vi = vr + kTile * kTile / 4;
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            vr[e] = make_int4(re[4 * e], re[4 * e + 1], re[4 * e + 2], re[4 * e + 3]);
+                            vi[e] = make_int4(im[4 * e], im[4 * e + 1], im[4 * e + 2], im[4 * e + 3]);
+                        }
+                    } else if (tr && kXposeBytes) {
+                        // row `lane` of the warp's 32 x 16 block -> pairs of rows,
+                        // 16 consecutive elements each, per instruction
+                        int32_t* xs = xchg + (warp - 2) * 32 * kXposeStride;
+                        const int rr = lane >> 4, cc = lane & 15;
+#pragma unroll 1
+                        for (int pl = 0; pl < 2; ++pl) {
+#pragma unroll
+                            for (int e = 0; e < 16; ++e) xs[lane * kXposeStride + e] = pl ? im[e] : re[e];
+                            __syncwarp();
+                            const size_t pb = tb + (size_t)pl * kTile * kTile + n0 + cc;
+#pragma unroll 4
+                            for (int s2 = 0; s2 < 16; ++s2) {
+                                const int row = 2 * s2 + rr;
+                                store1(it, pb + (size_t)(q * 32 + row) * kTile,
+                                       xs[row * kXposeStride + cc]);
+                            }
+                            __syncwarp();
+                        }
+                    } else if (tr) {
+                        store16<1>(it, tb + (size_t)m * kTile + n0, re, im);
+                    } else {
+                        store16<kTile>(it, tb + (size_t)n0 * kTile + m, re, im);
+                    }
+                }
+            } else if (!(kDiag3 && it.i == it.j)) {
 #pragma unroll 1
                 for (int n0 = 0; n0 < kEpiCols; n0 += 16) {
                     uint32_t r[4][16];   // R1, P2, P1, R2
@@ -415,7 +628,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         re[e] = (int32_t)(r[0][e] + r[3][e]);
                         im[e] = (int32_t)(r[2][e] - r[1][e]);
                     }
-                    store16(it, tb + (size_t)(col0 + n0) * kTile + m, re, im);
+                    store16<kTile>(it, tb + (size_t)(col0 + n0) * kTile + m, re, im);
                 }
             } else {
                 // Diagonal tile: TMEM holds R1 (columns 0-127), P2 (128-255) and
@@ -459,7 +672,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                                 re[e] = (int32_t)(r1[e] + r2[e]);
                                 im[e] = (int32_t)((uint32_t)p2t - p2[e]);
                             }
-                            store16(it, tb + (size_t)(col0 + n0) * kTile + m, re, im);
+                            store16<kTile>(it, tb + (size_t)(col0 + n0) * kTile + m, re, im);
                         }
                     }
                     named_bar_sync(kEpiBarrier, 32 * kEpiWarps);   // blocks consumed
@@ -854,6 +1067,35 @@ int xcorr_encode_map(CUtensorMap* map, const int8_t* planes, int32_t nant, int32
     return r == CUDA_SUCCESS ? MIXER_OK : MIXER_EINVAL;
 }
 
+int xcorr_encode_maps(CUtensorMap* maps, const int8_t* planes, int32_t nant, int32_t nch, int64_t kt,
+                      int64_t kend) {
+    int rc = xcorr_encode_map(&maps[0], planes, nant, nch, kt, kend);
+    if (rc != MIXER_OK) return rc;
+    EncodeFn enc = get_encode();
+    if (!enc) return MIXER_ECUDA;
+    // The ragged last block: tail_rows(nant) rows of both planes in one box,
+    // landing as [Xr rows ; Xi rows] (the 2 r16-row B operand).  Encoded for
+    // every array; unused when N is a multiple of 128.
+    const cuuint64_t dims[4] = {(cuuint64_t)kend, (cuuint64_t)nant, (cuuint64_t)nch, 2};
+    const cuuint64_t strides[3] = {(cuuint64_t)kt, (cuuint64_t)kt * nant,
+                                   (cuuint64_t)kt * nant * nch};
+    const cuuint32_t box[4] = {kKc, (cuuint32_t)tail_rows(nant), 1, 2};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(&maps[1], CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<int8_t*>(planes), dims,
+                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     kKc == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? MIXER_OK : MIXER_EINVAL;
+}
+
+// Dynamic shared memory of a launch: the transpose area only when it holds
+// ragged-block tiles (measured: the larger carve-out slows the int64
+// epilogue of other launches by up to 5 %).
+static int launch_smem(bool ragged) {
+    if (kDiag3) return kSmemBytes;
+    return kSmemBase + ((MIXER_XCORR_TAIL && ragged) ? kXposeBytes : 0);
+}
+
 static int set_smem_attr() {
     static uint64_t attr_set = 0;   // one bit per device ordinal
     int dev = 0;
@@ -951,13 +1193,13 @@ static int pair_launch(const CUtensorMap& map, int32_t nant, int32_t nch, int64_
 static int xcorr_launch(const int8_t* planes, int32_t nant, int32_t nch, int64_t kt, int64_t kbeg,
                         int64_t klen, int32_t mode, void* vis, int32_t max_ctas, int32_t* err,
                         cudaStream_t st) {
-    CUtensorMap map;
-    int rc = xcorr_encode_map(&map, planes, nant, nch, kt, kbeg + klen);
+    CUtensorMap maps[2];
+    int rc = xcorr_encode_maps(maps, planes, nant, nch, kt, kbeg + klen);
     if (rc != MIXER_OK) return rc;
     if (max_ctas != 1 && pairs_wanted((nant + kTile - 1) / kTile)) {
         const int clusters = pair_clusters();
         if (clusters > 0)
-            return pair_launch(map, nant, nch, kbeg, klen, mode, vis, max_ctas, err, clusters, st);
+            return pair_launch(maps[0], nant, nch, kbeg, klen, mode, vis, max_ctas, err, clusters, st);
     }
     rc = set_smem_attr();
     if (rc != MIXER_OK) return rc;
@@ -973,33 +1215,38 @@ static int xcorr_launch(const int8_t* planes, int32_t nant, int32_t nch, int64_t
     a.nwork = (int64_t)nch * a.ntiles;
     a.vis = vis;
     a.err = err;
+    a.ctr = nullptr;
     a.tmaps = nullptr;
     a.probs = nullptr;
     a.work = nullptr;
     int64_t grid = sm_count();
     if (max_ctas > 0 && max_ctas < grid) grid = max_ctas;
     if (a.nwork < grid) grid = a.nwork;
-    k_xcorr_tri<<<(unsigned)grid, kThreads, kSmemBytes, st>>>(map, a);
+    k_xcorr_tri<<<(unsigned)grid, kThreads, launch_smem(nant % kTile != 0), st>>>(maps[0], maps[1],
+                                                                                  a);
     MIXER_CK(cudaGetLastError());
     return MIXER_OK;
 }
 
 int xcorr_launch_table(const CUtensorMap* d_tmaps, const XcorrProblem* d_probs,
                        const XcorrWork* d_work, int64_t nwork, int grid, int32_t* err,
-                       cudaStream_t st) {
-    if (nwork <= 0 || grid <= 0) return MIXER_EINVAL;
+                       unsigned long long* ctr, bool ragged, cudaStream_t st) {
+    if (nwork <= 0 || grid <= 0 || !ctr) return MIXER_EINVAL;
     int rc = set_smem_attr();
     if (rc != MIXER_OK) return rc;
+    MIXER_CK(cudaMemsetAsync(ctr, 0, sizeof(*ctr), st));
     XcorrArgs a;
     memset(&a, 0, sizeof(a));
     a.nwork = nwork;
     a.err = err;
+    a.ctr = ctr;
     a.tmaps = d_tmaps;
     a.probs = d_probs;
     a.work = d_work;
     CUtensorMap unused;
     memset(&unused, 0, sizeof(unused));
-    k_xcorr_tri<<<(unsigned)(grid < nwork ? grid : nwork), kThreads, kSmemBytes, st>>>(unused, a);
+    k_xcorr_tri<<<(unsigned)(grid < nwork ? grid : nwork), kThreads, launch_smem(ragged), st>>>(
+        unused, unused, a);
     MIXER_CK(cudaGetLastError());
     return MIXER_OK;
 }

@@ -125,6 +125,40 @@ def test_xcorr_store_i32_matches_oracle(cuda, nant, nch, kt, kbeg, klen):
     assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("nant", [1, 15, 16, 17, 100, 129, 143, 160, 241, 255, 257, 300, 383, 1000])
+@pytest.mark.parametrize("mode", ["store", "acc32", "acc64"])
+def test_xcorr_ragged_last_block_matches_oracle(cuda, nant, mode):
+    """N not a multiple of 128: the last block's tiles run with that block on
+    the MMA's N side (N = 2 r16, r16 = rows rounded up to 16), the tiles left
+    of the diagonal as conjugate transposes written back transposed.  Every
+    rounding class of the last block, each mode, -128 rows in the ragged
+    block; store mode rewrites the padding rows (the cube starts as junk),
+    the accumulate modes add twice."""
+    import torch
+    rng = np.random.default_rng(nant * 3 + len(mode))
+    nch, kt = 2, 384
+    planes = _rand_planes(rng, nch, nant, kt)
+    planes[:, :, -min(nant, 5):, ::3] = -128
+    dpl = _t(planes, cuda)
+    n = mixer.vis_elems(nant, nch)
+    err = _zeros(1, torch.int32, cuda)
+    ref = oracle.vis_tile_pack(oracle.correlate(planes)).reshape(-1)
+    if mode == "store":
+        vis = torch.full((n,), 0x5A5A5A5A, dtype=torch.int32, device=cuda)
+        mixer.xcorr_tri(dpl, nant, nch, kt, 0, kt, mixer.VIS_STORE_I32, vis, err)
+        times = 1
+    else:
+        dt = torch.int64 if mode == "acc64" else torch.int32
+        md = mixer.VIS_ACC_I64 if mode == "acc64" else mixer.VIS_ACC_I32
+        vis = _zeros(n, dt, cuda)
+        for _ in range(2):
+            mixer.xcorr_tri(dpl, nant, nch, kt, 0, kt, md, vis, err)
+        times = 2
+    _sync()
+    assert int(err.item()) == 0
+    assert np.array_equal(vis.cpu().numpy().astype(np.int64), times * ref)
+
+
 def test_xcorr_accumulate_modes(cuda):
     import torch
     rng = np.random.default_rng(11)
