@@ -248,7 +248,10 @@ int mixer_batch_plan(mixer_batch* b, const int32_t* split_per_class, int32_t ncl
  * (longest-first, no split) by as much or the default is kept.  The ACC-mode
  * cubes accumulate every trial: zero them afterwards. */
 int mixer_batch_autotune(mixer_batch* b, int32_t reps, void* stream, float* best_ms);
-/* One launch of the current plan. */
+/* One launch of the current plan.  The launch's CTAs take the work items in
+ * list order from an item counter the batch owns (zeroed on `stream` before
+ * the launch, so a captured graph zeroes it too): runs or replays of ONE batch
+ * must not overlap on the GPU (they would also add into the same cubes). */
 int mixer_batch_run(mixer_batch* b, void* stream);
 /* Capture one launch of the current plan into a CUDA graph (stream must not be
  * the legacy default stream); replay it with mixer_batch_replay.  Re-planning
